@@ -1,0 +1,305 @@
+#!/usr/bin/env python3
+"""Benchmark of the colour-gradient LBM step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload: one 4096 x 4096 x 1 periodic box, static drop R = 400, operator P3 chi = 0.5,
+A = 0.225, tau = 1, beta = 0.8 (the single-case roofline configuration of the north star), stepped
+in FP32 shifted storage; the plain FP64 path (bit-identical to the reference) is measured on the
+same case beside it.  A "step" is one lattice-Boltzmann time step of the whole box.
+
+value   MLUPS (million lattice-node updates per second), device time from CUDA events on the
+        launching stream around exactly K steps, inputs resident in HBM.  The state (5.1 GB FP32,
+        10.2 GB FP64) is far larger than L2, so no flush is needed between steps.
+e2e     the same metric through the C ABI as a user runs a case: itlbm_case_create (the initial
+        profile is computed on the host and copied up), K steps with a diagnostic every 500 steps and
+        at the end (each one a device-to-host copy of the observables), wall clock.
+roofline algorithmic bytes per update: 38 populations read + 38 written (304 B in FP32, 608 B in
+        FP64) x nodes / mean kernel duration, against the measured copy bandwidth.
+cpu_baseline the reference's own step (Imm_OPS.cpp:252-287, compiled from its sources with its own
+        flags into oracle/_ref) on all host cores, on a bounded 1024 x 1024 sample.
+
+Multi-GPU: cases are independent, so N GPUs run N replicas with no collective (weak scaling);
+value is the sum of the ranks' node updates over the slowest rank's time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "oracle"))
+
+PEAKS = REPO / "MEASURED_PEAKS.json"
+HBM_FALLBACK = 6650.0
+
+
+def hbm_peak():
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+WORKLOADS = {
+    "drop4096": dict(nx=4096, ny=4096, radius=400.0, tipo=3, chi=0.5, xi=1.569988, A=0.225, tau=1.0,
+                     beta=0.8, kprof=2.0 * math.log(9.0) / 3.45),
+    "drop1024": dict(nx=1024, ny=1024, radius=100.0, tipo=3, chi=0.5, xi=1.569988, A=0.225, tau=1.0,
+                     beta=0.8, kprof=2.0 * math.log(9.0) / 3.45),
+}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def setup_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def allreduce_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_case(pkg, w, prec):
+    op = pkg.make_op(w["tipo"], w["chi"], w["xi"])
+    d = pkg.desc(w["nx"], w["ny"], op, tau=w["tau"], beta=w["beta"], A_fact=w["A"], radius=w["radius"],
+                 k_profile=w["kprof"], precision=prec)
+    return pkg.Case(d)
+
+
+def device_run(pkg, w, prec, steps, warmup, world, sample_clocks, local):
+    """MLUPS of exactly `steps` steps, CUDA events on the launching stream, max over ranks."""
+    import torch
+    c = make_case(pkg, w, prec)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    c.step(warmup, stream=sp)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local) if sample_clocks else None
+    if sampler:
+        sampler.__enter__()
+        time.sleep(0.3)
+    e0.record(stream)
+    c.step(steps, stream=sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__()
+    barrier(world)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ms_max = allreduce_max(ms, world)
+    n = w["nx"] * w["ny"]
+    c.close()
+    return n, ms, ms_max, (sampler.summary() if sampler else None)
+
+
+def e2e_run(pkg, w, prec, steps):
+    """A whole case through the C ABI with host buffers: create (host profile -> device), steps,
+    a diagnostic every 500 steps and at the end (device -> host), destroy.  Wall clock."""
+    import ctypes
+    t0 = time.perf_counter()
+    c = make_case(pkg, w, prec)
+    ndiag = 0
+    done = 0
+    while done < steps:
+        chunk = min(500, steps - done)
+        c.step(chunk, keep_aux=True)
+        done += chunk
+        c.diag_drop(done - 1)
+        ndiag += 1
+    c.close()
+    dt = time.perf_counter() - t0
+    n = w["nx"] * w["ny"]
+    h2d = 8 * n  # the initial profile rho^N(r) per node, double
+    d2h = ndiag * ctypes.sizeof(pkg.DropDiag)
+    return {"value": n * steps / dt / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "wall_s": dt}
+
+
+def cpu_baseline(threads=0):
+    import oracle
+    if not oracle.REF_DIR.joinpath("libref_ops_fast.so").exists():
+        return None
+    nx = 1024
+    steps = 8
+    mlups, dt, nthr = oracle.time_reference_step(nx, nx, steps=steps, warmup=1, threads=threads)
+    return {"value": mlups, "unit": "MLUPS", "cores": nthr, "kind": "reference",
+            "sample": f"reference step loop (Imm_OPS.cpp:252-287, oracle/_ref, its own flags), "
+                      f"{nx}x{nx} drop P3 chi=0.5, {steps} steps, {nthr} OpenMP threads, {dt:.1f} s"}
+
+
+def run_reference(args):
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    import oracle
+    w = WORKLOADS[args.workload]
+    nx = 1024  # bounded sample of the same workload (per-node work is size independent on a CPU)
+    threads = os.cpu_count() or 1
+    total = 0.0
+    tsum = 0.0
+    oracle.time_reference_step(nx, nx, steps=max(1, args.warmup), warmup=0, threads=threads)
+    mlups, dt, nthr = oracle.time_reference_step(nx, nx, steps=args.steps, warmup=0, threads=threads)
+    line = {"impl": "reference", "metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "sample_nx": nx, "sample_ny": nx},
+            "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": nthr, "kind": "reference",
+                             "sample": f"{nx}x{nx} sample of {args.workload}, {args.steps} steps"},
+            "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="drop4096", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    world, rank, local = setup_dist()
+    import torch
+    torch.cuda.set_device(local)
+    import oracle  # noqa: F401  (loads the package binding)
+    pkg = oracle.load_package()
+    w = WORKLOADS[args.workload]
+    peak, peak_kind = hbm_peak()
+
+    # headline: FP32 shifted storage
+    n, ms, ms_max, clocks = device_run(pkg, w, pkg.PREC_F32, args.steps, args.warmup, world, rank == 0, local)
+    mlups = allreduce_sum(n * args.steps, world) / (ms_max * 1e-3) / 1e6
+    bytes_lu = 304.0
+    achieved = bytes_lu * n * args.steps / (ms * 1e-3) / 1e9
+    # plain FP64 on the same case
+    n64, ms64, ms64_max, _ = device_run(pkg, w, pkg.PREC_F64, max(50, args.steps // 4), args.warmup,
+                                        world, False, local)
+    k64 = max(50, args.steps // 4)
+    mlups64 = allreduce_sum(n64 * k64, world) / (ms64_max * 1e-3) / 1e6
+    achieved64 = 608.0 * n64 * k64 / (ms64 * 1e-3) / 1e9
+
+    e2e = None if args.no_e2e else e2e_run(pkg, w, pkg.PREC_F32, args.steps)
+    if e2e and world > 1:
+        e2e["value"] = allreduce_sum(e2e["value"], world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        line = {
+            "metric": "MLUPS & % HBM roofline, batched FP32 vs plain FP64 on 1 B200; p99 case latency",
+            "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x1 static drop R={w['radius']:g}, "
+                                   f"P3 chi=0.5, A=0.225, tau=1, beta=0.8, FP32 shifted storage",
+                       "nodes": n, "l2": "state 5.1 GB/step (FP32) >> 126 MB L2: no flush needed",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "bytes_per_lu": bytes_lu},
+            "fp64_plain": {"value": mlups64, "unit": "MLUPS", "steps": k64,
+                           "roofline": {"achieved": achieved64, "frac": achieved64 / peak, "bytes_per_lu": 608.0}},
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

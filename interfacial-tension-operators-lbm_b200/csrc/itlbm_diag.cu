@@ -1,0 +1,917 @@
+// itlbm_diag.cu -- diagnostics of one case on the device (FP64 accumulation).
+//
+// The reference measures every PASSOS_DIAG steps on the host (Imm_OPS.cpp:293-342,
+// Imm_INCL.cpp:400-434).  Here every full-field pass is a grid-stride kernel whose threads
+// accumulate in FP64, reduce within the block by warp shuffles and write one partial per block; a
+// one-block kernel then reduces the partials in block order.  The order depends only on the size of
+// the case, so a case gives the same bits alone or in a batch.  The shell histogram of the logistic
+// fit is accumulated in 64-bit fixed point (2^-40), which makes its atomics order-independent too.
+// The scalar finalisation (centroid angle, fits, ratios) runs in single-thread kernels, so one
+// diagnostic is a chain of launches on one stream with a single copy of the result at the end.
+//
+// Passes of a drop diagnostic (post-collision populations P(x)_i = dst(x + c_i, i)):
+//   D1  calc_galilean's first loop (Galilean_diagnostics.cpp:31-60) and calc_drop_radius's first
+//       loop (Other_functions.cpp:89-178); writes rho_R, rho_B, u, phi per node
+//   F1  means, centroid, equimolar radius (Galilean_diagnostics.cpp:61-63, Other_functions.cpp:180-190)
+//   D2  calc_drop_radius's second loop (:211-249), calc_laplace_tension's loop (:488-526),
+//       calc_galilean's second loop (Galilean_diagnostics.cpp:68-87) and the shell histogram of
+//       calc_perfil_logistico (Other_functions.cpp:341-377)
+//   F2  pressures, sigma, axis ratio, line estimators (:530-553, Galilean_diagnostics.cpp:88-104)
+//   FIT calc_perfil_logistico's fit (Other_functions.cpp:381-445)
+//   MOD modos_interface (Operadores_tensao.cpp:382-449), one thread per ray
+#include "itlbm_site.cuh"
+
+#include <cfloat>
+
+namespace itlbm {
+
+namespace {
+
+constexpr int DT = 256;        // threads of the reduction kernels
+constexpr int MAXB = 148 * 8;  // at most this many partials per pass
+constexpr double FIX = 1099511627776.0;  // 2^40
+
+// Post-collision populations of node (x, y) in FP64.
+__device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int y, double *fR,
+                                          double *fB) {
+    const int xp = (x + 1 == c.nx) ? 0 : x + 1, xm = (x == 0) ? c.nx - 1 : x - 1;
+    const int yp = (y + 1 == c.ny) ? 0 : y + 1, ym = (y == 0) ? c.ny - 1 : y - 1;
+    if (c.prec == ITLBM_PREC_F64) {
+        const double *d = (const double *)c.buf[cur];
+        sfor<0, NV>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const int xs = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
+            const int ys = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
+            const long long o = (long long)ys * c.pitch + xs;
+            fR[i] = d[(long long)i * c.stride + o];
+            fB[i] = d[(long long)(NV + i) * c.stride + o];
+        });
+    } else {
+        const float *d = (const float *)c.buf[cur];
+        sfor<0, NV>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const int xs = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
+            const int ys = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
+            const long long o = (long long)ys * c.pitch + xs;
+            const double e = d[(long long)i * c.stride + o];
+            const double dd = d[(long long)(NV + i) * c.stride + o];
+            const double f = wgt<double>(i) * c.rho0 + e;
+            fR[i] = 0.5 * (f + dd);
+            fB[i] = 0.5 * (f - dd);
+        });
+    }
+}
+
+__device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
+
+// Block reduction of Q quantities: [0, NS) sums, [NS, NS+NM) maxima, the rest minima.  Writes the
+// block's result to out[0..Q).  Deterministic for a fixed block size.
+template <int Q, int NS, int NM>
+__device__ void block_reduce(double (&v)[Q], double *out) {
+    __shared__ double sh[DT / 32][Q];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        double a = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double b = __shfl_down_sync(0xffffffffu, a, o);
+            if (q < NS) a = a + b;
+            else if (q < NS + NM) a = (a < b) ? b : a;
+            else a = (b < a) ? b : a;
+        }
+        if (lane == 0) sh[warp][q] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < Q) {
+        const int q = threadIdx.x;
+        double a = sh[0][q];
+        for (int w = 1; w < DT / 32; w++) {
+            const double b = sh[w][q];
+            if (q < NS) a = a + b;
+            else if (q < NS + NM) a = (a < b) ? b : a;
+            else a = (b < a) ? b : a;
+        }
+        out[q] = a;
+    }
+    __syncthreads();
+}
+
+template <int Q, int NS, int NM>
+__device__ __forceinline__ void init_acc(double (&v)[Q]) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) v[q] = (q < NS) ? 0.0 : (q < NS + NM ? -DBL_MAX : DBL_MAX);
+}
+
+// Reduce nb partials (rows of Q) in block order into res[0..Q).
+template <int Q, int NS, int NM>
+__global__ void k_reduce(const double *__restrict__ part, int nb, double *__restrict__ res) {
+    double v[Q];
+    init_acc<Q, NS, NM>(v);
+    for (int b = threadIdx.x; b < nb; b += DT) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const double x = part[(long long)b * Q + q];
+            if (q < NS) v[q] = v[q] + x;
+            else if (q < NS + NM) v[q] = (v[q] < x) ? x : v[q];
+            else v[q] = (x < v[q]) ? x : v[q];
+        }
+    }
+    block_reduce<Q, NS, NM>(v, res);
+}
+
+// ---------------------------------------------------------------------------------------------
+// drop
+// ---------------------------------------------------------------------------------------------
+// D1 quantities
+enum {
+    A_MASS, A_MASSR, A_QXG, A_QYG, A_QZG, A_QRX, A_QRY, A_MASSA_R, A_MASSA_B, A_QXD, A_QYD, A_QZD,
+    A_U2, A_AREA, A_CXC, A_CXS, A_CYC, A_CYS, A_BAD, A_NEGT, A_NEGC, A_RUIM,  // sums (22)
+    A_UMAXD, A_MAXPHI,                                                        // maxima (2)
+    A_MINF, A_MINRHO, A_MINPHI,                                               // minima (3)
+    A_Q
+};
+constexpr int A_NS = 22, A_NM = 2;
+// D2 quantities
+enum {
+    B_SOMW, B_SOMWR, B_SXE, B_SWE, B_SXD, B_SWD, B_PIN, B_PIN2, B_POUT, B_POUT2, B_PCTR, B_NIN,
+    B_NOUT, B_NCTR, B_SREF, B_SMEAN, B_SLAB, B_WEIGHT, B_SX, B_SY, B_SXX, B_SYY, B_SXY, B_LW, B_LX,
+    B_RW, B_RX,                       // sums (27)
+    B_MAXREF, B_MAXMEAN, B_MAXLAB,    // maxima (3)
+    B_Q
+};
+constexpr int B_NS = 27, B_NM = 3;
+
+// device-side state of one drop diagnostic
+struct DropState {
+    double a[A_Q];
+    double b[B_Q];
+    int proceed;      // D1 passed (no bad node, positive masses)
+    int y_lin, y_line;
+    double r_in_max, r_out_min;
+    double fit[6];
+};
+
+__global__ void __launch_bounds__(DT) k_drop_d1(const CaseDev *__restrict__ cp, int cur,
+                                                int use_force, double *__restrict__ node,
+                                                double *__restrict__ part) {
+    const CaseDev &c = *cp;
+    const int nx = c.nx, ny = c.ny;
+    const long long n = (long long)nx * ny;
+    const double pi = 3.14159265358979323846;
+    const double tx = 2.0 * pi / (double)nx, ty = 2.0 * pi / (double)ny;
+    double v[A_Q];
+    init_acc<A_Q, A_NS, A_NM>(v);
+    for (long long p = blockIdx.x * (long long)DT + threadIdx.x; p < n; p += (long long)gridDim.x * DT) {
+        const int x = (int)(p % nx), y = (int)(p / nx);
+        double fR[NV], fB[NV];
+        post_pops(c, cur, x, y, fR, fB);
+        // calc_galilean, first loop
+        double rr = 0, rb = 0, mx = 0, my = 0, mz = 0;
+        int bad = 0;
+        sfor<0, NV>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const double fr = fR[i], fb = fB[i];
+            const double f = fr + fb;
+            if (!finite_d(fr) || !finite_d(fb)) ++bad;
+            v[A_MINF] = (f < v[A_MINF]) ? f : v[A_MINF];
+            if (f < -1.e-12) v[A_NEGT] += 1.0;
+            if (fr < -1.e-12) v[A_NEGC] += 1.0;
+            if (fb < -1.e-12) v[A_NEGC] += 1.0;
+            rr += fr;
+            rb += fb;
+            if constexpr (cx(i) == 1) mx += f;
+            if constexpr (cx(i) == -1) mx -= f;
+            if constexpr (cy(i) == 1) my += f;
+            if constexpr (cy(i) == -1) my -= f;
+            if constexpr (cz(i) == 1) mz += f;
+            if constexpr (cz(i) == -1) mz -= f;
+        });
+        const double rho = rr + rb;
+        double ux = 0, uy = 0, uz = 0, ph = 0;
+        bool ok = true;
+        if (!finite_d(rho) || rho <= 0 || !finite_d(mx) || !finite_d(my) || !finite_d(mz)) {
+            ++bad;
+            ok = false;
+        }
+        double F0 = 0, F1 = 0, F2 = 0;
+        if (ok && use_force) {
+            const long long o = (long long)y * c.pitch + x;
+            F0 = c.aux[o];
+            F1 = c.aux[c.stride + o];
+            F2 = c.aux[2 * c.stride + o];
+            if (!finite_d(F0) || !finite_d(F1) || !finite_d(F2)) {
+                ++bad;
+                ok = false;
+            } else {
+                mx -= 0.5 * F0;
+                my -= 0.5 * F1;
+                mz -= 0.5 * F2;
+            }
+        }
+        v[A_BAD] += bad;
+        if (ok) {
+            v[A_MINRHO] = (rho < v[A_MINRHO]) ? rho : v[A_MINRHO];
+            ux = mx / rho;
+            uy = my / rho;
+            uz = mz / rho;
+            ph = rr / rho;
+            v[A_MINPHI] = (ph < v[A_MINPHI]) ? ph : v[A_MINPHI];
+            v[A_MAXPHI] = (v[A_MAXPHI] < ph) ? ph : v[A_MAXPHI];
+            v[A_MASS] += rho;
+            v[A_MASSR] += rr;
+            v[A_QXG] += mx;
+            v[A_QYG] += my;
+            v[A_QZG] += mz;
+            v[A_QRX] += rr * ux;
+            v[A_QRY] += rr * uy;
+        }
+        node[p] = rr;
+        node[n + p] = rb;
+        node[2 * n + p] = ux;
+        node[3 * n + p] = uy;
+        node[4 * n + p] = uz;
+        node[5 * n + p] = ph;
+        // calc_drop_radius, first loop (calcula per colour, LBM_functions.cpp:1100-1171)
+        double mRx = 0, mRy = 0, mRz = 0, mBx = 0, mBy = 0, mBz = 0;
+        sfor<0, NV>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            if constexpr (cx(i) == 1) { mRx += fR[i]; mBx += fB[i]; }
+            if constexpr (cx(i) == -1) { mRx -= fR[i]; mBx -= fB[i]; }
+            if constexpr (cy(i) == 1) { mRy += fR[i]; mBy += fB[i]; }
+            if constexpr (cy(i) == -1) { mRy -= fR[i]; mBy -= fB[i]; }
+            if constexpr (cz(i) == 1) { mRz += fR[i]; mBz += fB[i]; }
+            if constexpr (cz(i) == -1) { mRz -= fR[i]; mBz -= fB[i]; }
+        });
+        const double rho_R = rr, rho_B = rb;
+        double vxR = 0, vyR = 0, vzR = 0, vxB = 0, vyB = 0, vzB = 0;
+        if (rho_R != 0.0) {
+            const double inv = 1.0 / rho_R;
+            vxR = mRx * inv; vyR = mRy * inv; vzR = mRz * inv;
+        }
+        if (rho_B != 0.0) {
+            const double inv = 1.0 / rho_B;
+            vxB = mBx * inv; vyB = mBy * inv; vzB = mBz * inv;
+        }
+        if (!(rho_R == rho_R) || !(rho_B == rho_B) || !(vxR == vxR) || !(vxB == vxB)) {
+            v[A_RUIM] += 1.0;
+            continue;
+        }
+        v[A_MASSA_R] += rho_R;
+        v[A_MASSA_B] += rho_B;
+        v[A_QXD] += rho_R * vxR + rho_B * vxB;
+        v[A_QYD] += rho_R * vyR + rho_B * vyB;
+        v[A_QZD] += rho_R * vzR + rho_B * vzB;
+        const double rh = rho_R + rho_B;
+        if (rh <= 0.0) continue;
+        double uxd = (rho_R * vxR + rho_B * vxB) / rh;
+        double uyd = (rho_R * vyR + rho_B * vyB) / rh;
+        double uzd = (rho_R * vzR + rho_B * vzB) / rh;
+        if (use_force) {
+            const long long o = (long long)y * c.pitch + x;
+            const double G0 = c.aux[o], G1 = c.aux[c.stride + o], G2 = c.aux[2 * c.stride + o];
+            uxd = uxd - 0.5 * G0 / rh;
+            uyd = uyd - 0.5 * G1 / rh;
+            uzd = uzd - 0.5 * G2 / rh;
+            v[A_QXD] -= 0.5 * G0;
+            v[A_QYD] -= 0.5 * G1;
+            v[A_QZD] -= 0.5 * G2;
+        }
+        const double u2 = uxd * uxd + uyd * uyd + uzd * uzd;
+        v[A_U2] += u2;
+        const double u = sqrt(u2);
+        if (u > v[A_UMAXD]) v[A_UMAXD] = u;
+        const double phi = rho_R / rh;
+        v[A_AREA] += phi;
+        v[A_CXC] += phi * cos(tx * x);
+        v[A_CXS] += phi * sin(tx * x);
+        v[A_CYC] += phi * cos(ty * y);
+        v[A_CYS] += phi * sin(ty * y);
+    }
+    block_reduce<A_Q, A_NS, A_NM>(v, part + (long long)blockIdx.x * A_Q);
+}
+
+__global__ void k_drop_f1(const CaseDev *__restrict__ cp, DropState *__restrict__ st,
+                          itlbm_drop_diag *__restrict__ d) {
+    const CaseDev &c = *cp;
+    const double *a = st->a;
+    const int nx = c.nx, ny = c.ny;
+    const double pi = 3.14159265358979323846;
+    d->bad = (int)a[A_BAD];
+    d->min_f = a[A_MINF] == DBL_MAX ? INFINITY : a[A_MINF];
+    d->min_rho = a[A_MINRHO] == DBL_MAX ? INFINITY : a[A_MINRHO];
+    d->min_phi = a[A_MINPHI] > 1.0 ? 1.0 : a[A_MINPHI];
+    d->max_phi = a[A_MAXPHI] < 0.0 ? 0.0 : a[A_MAXPHI];
+    d->negative_total = (long long)a[A_NEGT];
+    d->negative_color = (long long)a[A_NEGC];
+    d->axis_ratio = 1.0;
+    const double mass = a[A_MASS], mass_r = a[A_MASSR];
+    st->proceed = !(d->bad || !(mass > 0) || !(mass_r > 0));
+    d->ok = 0;
+    if (!st->proceed) return;
+    d->mean_x = a[A_QXG] / mass;
+    d->mean_y = a[A_QYG] / mass;
+    d->mean_z = a[A_QZG] / mass;
+    d->drop_x = a[A_QRX] / mass_r;
+    d->drop_y = a[A_QRY] / mass_r;
+    // calc_drop_radius, Other_functions.cpp:180-190 (nz = 1, cilindro)
+    const double tx = 2.0 * pi / (double)nx, ty = 2.0 * pi / (double)ny;
+    double x0 = atan2(a[A_CXS], a[A_CXC]) / tx;
+    if (x0 < 0.0) x0 += nx;
+    double y0 = atan2(a[A_CYS], a[A_CYC]) / ty;
+    if (y0 < 0.0) y0 += ny;
+    const double area = a[A_AREA];
+    const double raio = (area > 0.0) ? sqrt(area / (pi * 1.0)) : 0.0;
+    d->x0 = x0;
+    d->y0 = y0;
+    d->area = area;
+    d->raio = raio;
+    d->massa_R = a[A_MASSA_R];
+    d->massa_B = a[A_MASSA_B];
+    d->qx = a[A_QXD];
+    d->qy = a[A_QYD];
+    d->qz = a[A_QZD];
+    const int n_fluid = nx * ny;
+    d->n_fluid = n_fluid;
+    d->n_ruim = (int)a[A_RUIM];
+    d->u_max = a[A_UMAXD] < 0 ? 0.0 : a[A_UMAXD];
+    d->u_rms = (n_fluid > 0) ? sqrt(a[A_U2] / (double)n_fluid) : 0.0;
+    int y_lin = (int)(y0 + 0.5);
+    if (y_lin >= ny) y_lin -= ny;
+    st->y_lin = y_lin;
+    st->y_line = ((int)floor(y0 + 0.5)) % ny;
+    // calc_laplace_tension region limits, Other_functions.cpp:471-479 (frac 0.5 / 2.0, 3.45)
+    double r_in_max = 0.5 * raio, r_out_min = 2.0 * raio;
+    if (r_out_min < raio + 4.0 * 3.45) r_out_min = raio + 4.0 * 3.45;
+    const double r_caixa = 0.45 * (double)((nx < ny) ? nx : ny);
+    if (r_out_min > r_caixa) r_out_min = r_caixa;
+    st->r_in_max = r_in_max;
+    st->r_out_min = r_out_min;
+}
+
+__device__ __forceinline__ double min_image(double dx, int L) {
+    if (dx > 0.5 * L) dx -= L;
+    if (dx < -0.5 * L) dx += L;
+    return dx;
+}
+__device__ __forceinline__ double gi_image(double dx, double L) { return dx - L * floor(dx / L + 0.5); }
+
+__global__ void __launch_bounds__(DT) k_drop_d2(const CaseDev *__restrict__ cp,
+                                                const DropState *__restrict__ st,
+                                                const itlbm_drop_diag *__restrict__ d, double v0,
+                                                const double *__restrict__ node,
+                                                double *__restrict__ part,
+                                                unsigned long long *__restrict__ shell, int nshell) {
+    if (!st->proceed) return;
+    const CaseDev &c = *cp;
+    const int nx = c.nx, ny = c.ny;
+    const long long n = (long long)nx * ny;
+    const double x0 = d->x0, y0 = d->y0;
+    const double mean_x = d->mean_x, mean_y = d->mean_y, mean_z = d->mean_z;
+    const int y_lin = st->y_lin, y_line = st->y_line;
+    const double r_in_max = st->r_in_max, r_out_min = st->r_out_min;
+    double v[B_Q];
+    init_acc<B_Q, B_NS, B_NM>(v);
+    for (long long p = blockIdx.x * (long long)DT + threadIdx.x; p < n; p += (long long)gridDim.x * DT) {
+        const int x = (int)(p % nx), y = (int)(p / nx);
+        const double rho_R = node[p], rho_B = node[n + p];
+        const double ux = node[2 * n + p], uy = node[3 * n + p], uz = node[4 * n + p];
+        const double phg = node[5 * n + p];
+        // calc_drop_radius, second loop
+        const double dx = min_image((double)x - x0, nx), dy = min_image((double)y - y0, ny);
+        const double r = sqrt(dx * dx + dy * dy + 0.0 * 0.0);
+        const double w = rho_R * rho_B;
+        v[B_SOMW] += w;
+        v[B_SOMWR] += w * r;
+        if (y == y_lin) {
+            if (dx < 0.0) { v[B_SXE] += w * (double)x; v[B_SWE] += w; }
+            else { v[B_SXD] += w * (double)x; v[B_SWD] += w; }
+        }
+        // calc_laplace_tension
+        const double pr = (1. / 3.) * (rho_R + rho_B);
+        if (r < r_in_max) { v[B_PIN] += pr; v[B_PIN2] += pr * pr; v[B_NIN] += 1.0; }
+        else if (r >= r_out_min) { v[B_POUT] += pr; v[B_POUT2] += pr * pr; v[B_NOUT] += 1.0; }
+        if (r < 1.5) { v[B_PCTR] += pr; v[B_NCTR] += 1.0; }
+        // calc_galilean, second loop
+        const double a2 = (ux - v0) * (ux - v0) + uy * uy + uz * uz;
+        const double b2 = (ux - mean_x) * (ux - mean_x) + (uy - mean_y) * (uy - mean_y) +
+                          (uz - mean_z) * (uz - mean_z);
+        const double c2 = ux * ux + uy * uy + uz * uz;
+        v[B_SREF] += a2;
+        v[B_SMEAN] += b2;
+        v[B_SLAB] += c2;
+        const double sa = sqrt(a2), sb = sqrt(b2), sc = sqrt(c2);
+        v[B_MAXREF] = (v[B_MAXREF] < sa) ? sa : v[B_MAXREF];
+        v[B_MAXMEAN] = (v[B_MAXMEAN] < sb) ? sb : v[B_MAXMEAN];
+        v[B_MAXLAB] = (v[B_MAXLAB] < sc) ? sc : v[B_MAXLAB];
+        const double gx = gi_image(x - x0, nx), gy = gi_image(y - y0, ny);
+        v[B_WEIGHT] += phg;
+        v[B_SX] += phg * gx;
+        v[B_SY] += phg * gy;
+        v[B_SXX] += phg * gx * gx;
+        v[B_SYY] += phg * gy * gy;
+        v[B_SXY] += phg * gx * gy;
+        if (y == y_line) {
+            const double wl = rho_R * rho_B;
+            if (gx < 0) { v[B_LW] += wl; v[B_LX] += wl * gx; }
+            else { v[B_RW] += wl; v[B_RX] += wl * gx; }
+        }
+        // calc_perfil_logistico shell histogram (half-node shells)
+        const double rho = rho_R + rho_B;
+        if (!(rho <= 1.0e-30)) {
+            const int k = (int)(r / 0.5);
+            if (k >= 0 && k < nshell) {
+                const long long fx = __double2ll_rn((rho_R / rho) * FIX);
+                atomicAdd(&shell[k], (unsigned long long)fx);
+                atomicAdd(&shell[nshell + k], 1ULL);
+            }
+        }
+    }
+    block_reduce<B_Q, B_NS, B_NM>(v, part + (long long)blockIdx.x * B_Q);
+}
+
+__global__ void k_drop_f2(const CaseDev *__restrict__ cp, DropState *__restrict__ st,
+                          itlbm_drop_diag *__restrict__ d, int step, double v0, double x_ini,
+                          double y_ini, const double *__restrict__ node) {
+    if (!st->proceed) return;
+    const CaseDev &c = *cp;
+    const int nx = c.nx, ny = c.ny;
+    const long long n = (long long)nx * ny;
+    const double *b = st->b;
+    d->raio_grad = (b[B_SOMW] > 0.0) ? b[B_SOMWR] / b[B_SOMW] : 0.0;
+    const double raio_linha_d =
+        (b[B_SWE] > 0.0 && b[B_SWD] > 0.0) ? 0.5 * (b[B_SXD] / b[B_SWD] - b[B_SXE] / b[B_SWE]) : 0.0;
+    const int n_in = (int)b[B_NIN], n_out = (int)b[B_NOUT], n_ctr = (int)b[B_NCTR];
+    const double p_in = (n_in > 0) ? b[B_PIN] / (double)n_in : 0.0;
+    const double p_out = (n_out > 0) ? b[B_POUT] / (double)n_out : 0.0;
+    const double var_in = (n_in > 0) ? b[B_PIN2] / (double)n_in - p_in * p_in : 0.0;
+    const double var_out = (n_out > 0) ? b[B_POUT2] / (double)n_out - p_out * p_out : 0.0;
+    d->p_in = p_in;
+    d->sd_in = (var_in > 0.0) ? sqrt(var_in) : 0.0;
+    d->p_out = p_out;
+    d->sd_out = (var_out > 0.0) ? sqrt(var_out) : 0.0;
+    d->n_in = n_in;
+    d->n_out = n_out;
+    d->delta_p = p_in - p_out;
+    d->sigma = 1.0 * d->raio * d->delta_p;
+    d->p_centro = (n_ctr > 0) ? b[B_PCTR] / (double)n_ctr : 0.0;
+    d->p_canto = (1. / 3.) * (node[0] + node[n]);  // pos == 0
+    d->sigma_linha = 1.0 * raio_linha_d * (d->p_centro - d->p_canto);
+    d->raio_linha = raio_linha_d;
+    // calc_galilean, Galilean_diagnostics.cpp:88-104
+    const int nn = nx * ny;
+    d->max_ref = b[B_MAXREF] < 0 ? 0.0 : b[B_MAXREF];
+    d->max_mean = b[B_MAXMEAN] < 0 ? 0.0 : b[B_MAXMEAN];
+    d->max_lab = b[B_MAXLAB] < 0 ? 0.0 : b[B_MAXLAB];
+    d->rms_ref = sqrt(b[B_SREF] / nn);
+    d->rms_mean = sqrt(b[B_SMEAN] / nn);
+    d->rms_lab = sqrt(b[B_SLAB] / nn);
+    const double weight = b[B_WEIGHT], sx = b[B_SX], sy = b[B_SY];
+    const double xx = b[B_SXX] / weight - (sx / weight) * (sx / weight);
+    const double yy = b[B_SYY] / weight - (sy / weight) * (sy / weight);
+    const double xy = b[B_SXY] / weight - (sx / weight) * (sy / weight), trace = xx + yy;
+    const double disc = sqrt((xx - yy) * (xx - yy) + 4 * xy * xy);
+    d->axis_ratio = (trace > disc) ? sqrt((trace + disc) / (trace - disc)) : INFINITY;
+    d->center_dx = gi_image(d->x0 - (x_ini + v0 * step), nx);
+    d->center_dy = gi_image(d->y0 - y_ini, ny);
+    d->x_unwrapped = x_ini + v0 * step + d->center_dx;
+    d->raio_linha = (b[B_LW] > 0 && b[B_RW] > 0) ? 0.5 * (b[B_RX] / b[B_RW] - b[B_LX] / b[B_LW]) : 0;
+    const int corner_x = ((int)floor(d->x0 + 0.5) + nx / 2) % nx;
+    const int corner_y = ((int)floor(d->y0 + 0.5) + ny / 2) % ny;
+    const long long pc = corner_x + (long long)nx * corner_y;
+    d->p_canto = node[pc] * (1. / 3.) + node[n + pc] * (1. / 3.);
+    d->sigma_linha = d->raio_linha * (d->p_centro - d->p_canto);
+    d->u_max = d->max_ref;
+    d->u_rms = d->rms_ref;
+    d->ok = isfinite(d->sigma) && isfinite(d->max_ref) && isfinite(d->axis_ratio);
+    st->proceed = d->ok;
+}
+
+// calc_perfil_logistico's fit over the shells (one block)
+__global__ void __launch_bounds__(DT) k_drop_fit(DropState *__restrict__ st,
+                                                 itlbm_drop_diag *__restrict__ d,
+                                                 const unsigned long long *__restrict__ shell,
+                                                 int nshell) {
+    if (!st->proceed) return;
+    const double eps = 1.0e-30, d_casca = 0.5;
+    double v[6];
+    init_acc<6, 6, 0>(v);
+    for (int k = threadIdx.x; k < nshell; k += DT) {
+        const double sn = (double)shell[nshell + k];
+        if (sn < 1.0) continue;
+        const double sphi = (double)(long long)shell[k] / FIX;
+        const double phi = sphi / sn;
+        if (phi <= 0.02 || phi >= 0.98) continue;
+        const double r = ((double)k + 0.5) * d_casca;
+        const double l = log(phi / (1.0 - phi));
+        v[0] += 1.0;
+        v[1] += r;
+        v[2] += l;
+        v[3] += r * r;
+        v[4] += r * l;
+        v[5] += 1.0;
+    }
+    __shared__ double res[6];
+    block_reduce<6, 6, 0>(v, res);
+    const double S = res[0], Sr = res[1], Sl = res[2], Srr = res[3], Srl = res[4];
+    const int n_usadas = (int)res[5];
+    double K = 0.0, r_meio = 0.0, a = 0.0, bb = 0.0;
+    bool fit = false;
+    if (n_usadas >= 3) {
+        const double den = S * Srr - Sr * Sr;
+        if (fabs(den) > eps) {
+            a = (S * Srl - Sr * Sl) / den;
+            bb = (Sl - a * Sr) / S;
+            K = -a;
+            if (fabs(a) > eps) r_meio = -bb / a;
+            fit = true;
+        }
+    }
+    double m[1] = {0.0};
+    if (fit) {
+        for (int k = threadIdx.x; k < nshell; k += DT) {
+            const double sn = (double)shell[nshell + k];
+            if (sn < 1.0) continue;
+            const double phi = ((double)(long long)shell[k] / FIX) / sn;
+            if (phi <= 0.02 || phi >= 0.98) continue;
+            const double r = ((double)k + 0.5) * d_casca;
+            const double dd = fabs(log(phi / (1.0 - phi)) - (a * r + bb));
+            if (dd > m[0]) m[0] = dd;
+        }
+    }
+    __shared__ double mres[1];
+    block_reduce<1, 0, 1>(m, mres);
+    if (threadIdx.x == 0) {
+        d->K_perfil = K;
+        d->r_perfil = r_meio;
+        d->res_perfil = fit ? mres[0] : 0.0;
+        d->esp_perfil = (K > eps) ? 2.0 * log(9.0) / K : 0.0;
+        d->n_perfil = n_usadas;
+    }
+}
+
+// modos_interface: one thread per ray, bisection on the bilinear rho^N field
+__device__ double fase_em(const double *__restrict__ node, long long n, int nx, int ny, double x,
+                          double y) {
+    if (!isfinite(x) || !isfinite(y)) return 0.0;  // keeps every index below in range
+    x = x - nx * floor(x / nx);
+    y = y - ny * floor(y / ny);
+    const int i0 = (int)floor(x), j0 = (int)floor(y);
+    const double tx = x - i0, ty = y - j0;
+    double v = 0.0;
+    for (int dj = 0; dj < 2; dj++)
+        for (int di = 0; di < 2; di++) {
+            const int ii = ((i0 + di) % nx + nx) % nx, jj = ((j0 + dj) % ny + ny) % ny;
+            const long long p = ii + (long long)jj * nx;
+            const double rR = node[p], rB = node[n + p];
+            const double wgt2 = (di ? tx : 1 - tx) * (dj ? ty : 1 - ty);
+            v += wgt2 * (rR - rB) / (rR + rB);
+        }
+    return v;
+}
+
+__global__ void __launch_bounds__(ITLBM_N_ANG) k_drop_modes(const CaseDev *__restrict__ cp,
+                                                            const DropState *__restrict__ st,
+                                                            itlbm_drop_diag *__restrict__ d,
+                                                            const double *__restrict__ node) {
+    if (!st->proceed) return;
+    const CaseDev &c = *cp;
+    const int nx = c.nx, ny = c.ny;
+    const long long n = (long long)nx * ny;
+    const int N_ANG = ITLBM_N_ANG;
+    const double x0 = d->x0, y0 = d->y0, R_est = d->raio;
+    const int k = threadIdx.x;
+    const double th = 2.0 * 3.14159265358979323846 * k / N_ANG, ct = cos(th), st_ = sin(th);
+    double a = 0.3 * R_est, b = 1.7 * R_est;
+    const double fa = fase_em(node, n, nx, ny, x0 + a * ct, y0 + a * st_);
+    for (int it = 0; it < 60; it++) {
+        const double mid = 0.5 * (a + b);
+        const double fm = fase_em(node, n, nx, ny, x0 + mid * ct, y0 + mid * st_);
+        if ((fm > 0) == (fa > 0)) a = mid;
+        else b = mid;
+    }
+    const double r = 0.5 * (a + b);
+    __shared__ double rs[ITLBM_N_ANG];
+    rs[k] = r;
+    __syncthreads();
+    if (k == 0) {
+        // sums in ray order, as the reference loop
+        double c2 = 0, s2 = 0, c4 = 0, s4 = 0, c8 = 0, s8 = 0, soma = 0, rmin = 1e30, rmax = 0;
+        for (int j = 0; j < N_ANG; j++) {
+            const double t = 2.0 * 3.14159265358979323846 * j / N_ANG, rr = rs[j];
+            soma += rr;
+            c2 += rr * cos(2 * t);
+            s2 += rr * sin(2 * t);
+            c4 += rr * cos(4 * t);
+            s4 += rr * sin(4 * t);
+            c8 += rr * cos(8 * t);
+            s8 += rr * sin(8 * t);
+            rmin = fmin(rmin, rr);
+            rmax = fmax(rmax, rr);
+        }
+        d->R0 = soma / N_ANG;
+        d->a2 = 2.0 * sqrt(c2 * c2 + s2 * s2) / N_ANG / d->R0;
+        d->a4 = 2.0 * sqrt(c4 * c4 + s4 * s4) / N_ANG / d->R0;
+        d->a8 = 2.0 * sqrt(c8 * c8 + s8 * s8) / N_ANG / d->R0;
+        d->rmin = rmin;
+        d->rmax = rmax;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// inclined strip: mede_inclinada (Imm_INCL.cpp:85-189)
+// ---------------------------------------------------------------------------------------------
+enum {
+    S_SIGPOP, S_INTGRAD, S_MASSR, S_MASSB, S_QX, S_QY, S_SFX, S_SFY, S_U2, S_SX, S_SY, S_SXX, S_SXY,
+    S_NFIT, S_RUIM, S_NEGT, S_NEGC,  // sums (17)
+    S_UMAX, S_UNMAX, S_UTMAX,        // maxima (3)
+    S_MINF,                          // minimum (1)
+    S_Q
+};
+constexpr int S_NS = 17, S_NM = 3;
+
+struct StripState {
+    double a[S_Q];
+    double K, a0;
+    int fit;
+    double res[1];
+};
+
+__device__ __forceinline__ double dist_central(int x, int y, int p, int q, int N) {
+    const double m = sqrt((double)(p * p + q * q));
+    long long s = ((long long)p * x + (long long)q * y) % N;
+    if (s < 0) s += N;
+    double d = ((double)s - 0.5 * N);
+    if (d >= 0.5 * N) d -= N;
+    if (d < -0.5 * N) d += N;
+    return -d / m;
+}
+
+__global__ void __launch_bounds__(DT) k_strip_s1(const CaseDev *__restrict__ cp, int cur, int p,
+                                                 int q, int use_force, double *__restrict__ part) {
+    const CaseDev &c = *cp;
+    const int N = c.nx;
+    const long long n = (long long)N * N;
+    const double m = sqrt((double)(p * p + q * q));
+    const double nx_ = p / m, ny_ = q / m, tx_ = -ny_, ty_ = nx_;
+    double v[S_Q];
+    init_acc<S_Q, S_NS, S_NM>(v);
+    for (long long t = blockIdx.x * (long long)DT + threadIdx.x; t < n; t += (long long)gridDim.x * DT) {
+        const int x = (int)(t % N), y = (int)(t / N);
+        double fR[NV], fB[NV];
+        post_pops(c, cur, x, y, fR, fB);
+        double rR = 0, rB = 0, jx = 0, jy = 0, Pxx = 0, Pyy = 0, Pxy = 0, Pzz = 0;
+        sfor<0, NV>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const double f = fR[i] + fB[i];
+            if (!finite_d(fR[i]) || !finite_d(fB[i])) v[S_RUIM] += 1.0;
+            if (f < -1e-12) v[S_NEGT] += 1.0;
+            if (fR[i] < -1e-12) v[S_NEGC] += 1.0;
+            if (fB[i] < -1e-12) v[S_NEGC] += 1.0;
+            v[S_MINF] = (f < v[S_MINF]) ? f : v[S_MINF];
+            rR += fR[i];
+            rB += fB[i];
+            if constexpr (cx(i) == 1) jx += f;
+            if constexpr (cx(i) == -1) jx -= f;
+            if constexpr (cy(i) == 1) jy += f;
+            if constexpr (cy(i) == -1) jy -= f;
+            if constexpr (cx(i) != 0) Pxx += f;
+            if constexpr (cy(i) != 0) Pyy += f;
+            if constexpr (cx(i) * cy(i) == 1) Pxy += f;
+            if constexpr (cx(i) * cy(i) == -1) Pxy -= f;
+            if constexpr (cz(i) != 0) Pzz += f;
+        });
+        const double rho = rR + rB;
+        if (!(rho > 0)) {
+            v[S_RUIM] += 1.0;
+            continue;
+        }
+        const long long o = (long long)y * c.pitch + x;
+        if (use_force) {
+            const double F0 = c.aux[o], F1 = c.aux[c.stride + o];
+            jx -= 0.5 * F0;
+            jy -= 0.5 * F1;
+            v[S_SFX] += F0;
+            v[S_SFY] += F1;
+        }
+        const double ux = jx / rho, uy = jy / rho;
+        v[S_MASSR] += rR;
+        v[S_MASSB] += rB;
+        v[S_QX] += jx;
+        v[S_QY] += jy;
+        const double u = hypot(ux, uy), un = fabs(ux * nx_ + uy * ny_), ut = fabs(ux * tx_ + uy * ty_);
+        v[S_UMAX] = (v[S_UMAX] < u) ? u : v[S_UMAX];
+        v[S_UNMAX] = (v[S_UNMAX] < un) ? un : v[S_UNMAX];
+        v[S_UTMAX] = (v[S_UTMAX] < ut) ? ut : v[S_UTMAX];
+        v[S_U2] += u * u;
+        const double Pnn = nx_ * nx_ * Pxx + 2 * nx_ * ny_ * Pxy + ny_ * ny_ * Pyy;
+        const double Ptt = tx_ * tx_ * Pxx + 2 * tx_ * ty_ * Pxy + ty_ * ty_ * Pyy;
+        v[S_SIGPOP] += Pnn - 0.5 * (Ptt + Pzz);
+        v[S_INTGRAD] += c.aux[3 * c.stride + o];
+        const double dd = dist_central(x, y, p, q, N);
+        const double cR = rR / rho;
+        if (cR > 0.02 && cR < 0.98 && fabs(dd) < 8.0) {
+            const double l = log(cR / (1.0 - cR));
+            v[S_SX] += dd;
+            v[S_SY] += l;
+            v[S_SXX] += dd * dd;
+            v[S_SXY] += dd * l;
+            v[S_NFIT] += 1.0;
+        }
+    }
+    block_reduce<S_Q, S_NS, S_NM>(v, part + (long long)blockIdx.x * S_Q);
+}
+
+__global__ void k_strip_f1(const CaseDev *__restrict__ cp, StripState *__restrict__ st, int p, int q,
+                           itlbm_strip_diag *__restrict__ r) {
+    const int N = cp->nx;
+    const double *a = st->a;
+    const double m = sqrt((double)(p * p + q * q));
+    const double comprimento = 2.0 * N * m;
+    r->sigma_pop = a[S_SIGPOP] / comprimento;
+    r->int_grad = a[S_INTGRAD] / comprimento;
+    r->massa_R = a[S_MASSR];
+    r->massa_B = a[S_MASSB];
+    r->qx = a[S_QX];
+    r->qy = a[S_QY];
+    r->SFx = a[S_SFX];
+    r->SFy = a[S_SFY];
+    r->u_max = a[S_UMAX] < 0 ? 0.0 : a[S_UMAX];
+    r->un_max = a[S_UNMAX] < 0 ? 0.0 : a[S_UNMAX];
+    r->ut_max = a[S_UTMAX] < 0 ? 0.0 : a[S_UTMAX];
+    r->min_f = a[S_MINF] == DBL_MAX ? 1e300 : a[S_MINF];
+    r->neg_total = (long long)a[S_NEGT];
+    r->neg_cor = (long long)a[S_NEGC];
+    r->n_ruim = (int)a[S_RUIM];
+    r->u_rms = sqrt(a[S_U2] / (N * N));
+    const int nfit = (int)a[S_NFIT];
+    r->n_ajuste = nfit;
+    st->fit = 0;
+    r->K = 0;
+    r->d0 = 0;
+    r->res = 0;
+    if (nfit > 3) {
+        const double Sx = a[S_SX], Sy = a[S_SY], Sxx = a[S_SXX], Sxy = a[S_SXY];
+        const double K = (nfit * Sxy - Sx * Sy) / (nfit * Sxx - Sx * Sx);
+        const double a0 = (Sy - K * Sx) / nfit;
+        r->K = K;
+        r->d0 = -a0 / K;
+        st->K = K;
+        st->a0 = a0;
+        st->fit = 1;
+    }
+    r->ok = (r->n_ruim == 0 && isfinite(r->u_max));
+}
+
+__global__ void __launch_bounds__(DT) k_strip_s2(const CaseDev *__restrict__ cp, int cur, int p,
+                                                 int q, const StripState *__restrict__ st,
+                                                 double *__restrict__ part) {
+    double m[1] = {0.0};
+    if (st->fit) {
+        const CaseDev &c = *cp;
+        const int N = c.nx;
+        const long long n = (long long)N * N;
+        const double K = st->K, a0 = st->a0;
+        for (long long t = blockIdx.x * (long long)DT + threadIdx.x; t < n;
+             t += (long long)gridDim.x * DT) {
+            const int x = (int)(t % N), y = (int)(t / N);
+            double fR[NV], fB[NV];
+            post_pops(c, cur, x, y, fR, fB);
+            double rR = 0, rB = 0;
+            for (int i = 0; i < NV; i++) {
+                rR += fR[i];
+                rB += fB[i];
+            }
+            const double rho = rR + rB;
+            if (!(rho > 0)) continue;
+            const double dd = dist_central(x, y, p, q, N);
+            const double cR = rR / rho;
+            if (cR > 0.02 && cR < 0.98 && fabs(dd) < 8.0) {
+                const double e = fabs(log(cR / (1.0 - cR)) - (a0 + K * dd));
+                if (e > m[0]) m[0] = e;
+            }
+        }
+    }
+    block_reduce<1, 0, 1>(m, part + blockIdx.x);
+}
+
+__global__ void k_strip_f2(StripState *__restrict__ st, itlbm_strip_diag *__restrict__ r) {
+    if (st->fit) r->res = st->res[0] < 0 ? 0.0 : st->res[0];
+}
+
+// per-node fields of the post-collision state (rec_density / rec_velocity / perfil.dat)
+__global__ void k_fields(const CaseDev *__restrict__ cp, int cur, int use_force, double *rR_out,
+                         double *rB_out, double *ux_out, double *uy_out, double *uz_out) {
+    const CaseDev &c = *cp;
+    const int nx = c.nx;
+    const long long n = (long long)nx * c.ny;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % nx), y = (int)(p / nx);
+        double fR[NV], fB[NV];
+        post_pops(c, cur, x, y, fR, fB);
+        double rr = 0, rb = 0, mx = 0, my = 0, mz = 0;
+        for (int i = 0; i < NV; i++) {
+            const double f = fR[i] + fB[i];
+            rr += fR[i];
+            rb += fB[i];
+            mx += f * cx(i);
+            my += f * cy(i);
+            mz += f * cz(i);
+        }
+        const double rho = rr + rb;
+        if (use_force && rho > 0.0) {
+            const long long o = (long long)y * c.pitch + x;
+            mx -= 0.5 * c.aux[o];
+            my -= 0.5 * c.aux[c.stride + o];
+            mz -= 0.5 * c.aux[2 * c.stride + o];
+        }
+        if (rR_out) rR_out[p] = rr;
+        if (rB_out) rB_out[p] = rb;
+        if (ux_out) ux_out[p] = mx / rho;
+        if (uy_out) uy_out[p] = my / rho;
+        if (uz_out) uz_out[p] = mz / rho;
+    }
+}
+
+int nblocks_for(long long n) {
+    long long b = (n + DT - 1) / DT;
+    if (b > MAXB) b = MAXB;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+cudaError_t diag_alloc(DiagScratch &s, int nx, int ny) {
+    const int n = nx * ny;
+    const int nshell = (int)(sqrt((double)(nx * nx + ny * ny + 1)) / 0.5) + 2;
+    if (s.node && s.n == n && s.nshell == nshell) return cudaSuccess;
+    diag_free(s);
+    s.n = n;
+    s.nblocks = nblocks_for(n);
+    s.nshell = nshell;
+    cudaError_t e;
+    if ((e = cudaMalloc(&s.node, sizeof(double) * 6 * (size_t)n)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&s.part, sizeof(double) * 32 * (size_t)MAXB)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&s.shell, sizeof(long long) * 2 * (size_t)nshell)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&s.state, sizeof(DropState) + sizeof(StripState) + 64)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&s.out, sizeof(itlbm_drop_diag) + sizeof(itlbm_strip_diag) + 64)) != cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
+
+void diag_free(DiagScratch &s) {
+    if (s.node) cudaFree(s.node);
+    if (s.part) cudaFree(s.part);
+    if (s.shell) cudaFree(s.shell);
+    if (s.state) cudaFree(s.state);
+    if (s.out) cudaFree(s.out);
+    s = DiagScratch();
+}
+
+cudaError_t launch_diag_drop(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
+                             int step, double v0, double x_ini, double y_ini, bool use_force,
+                             itlbm_drop_diag *out_dev, cudaStream_t st) {
+    DropState *ds = (DropState *)s.state;
+    const int nb = s.nblocks;
+    cudaMemsetAsync(out_dev, 0, sizeof(itlbm_drop_diag), st);
+    cudaMemsetAsync(s.shell, 0, sizeof(long long) * 2 * (size_t)s.nshell, st);
+    k_drop_d1<<<nb, DT, 0, st>>>(c_dev, cur, use_force ? 1 : 0, s.node, s.part);
+    k_reduce<A_Q, A_NS, A_NM><<<1, DT, 0, st>>>(s.part, nb, ds->a);
+    k_drop_f1<<<1, 1, 0, st>>>(c_dev, ds, out_dev);
+    k_drop_d2<<<nb, DT, 0, st>>>(c_dev, ds, out_dev, v0, s.node, s.part,
+                                 (unsigned long long *)s.shell, s.nshell);
+    k_reduce<B_Q, B_NS, B_NM><<<1, DT, 0, st>>>(s.part, nb, ds->b);
+    k_drop_f2<<<1, 1, 0, st>>>(c_dev, ds, out_dev, step, v0, x_ini, y_ini, s.node);
+    k_drop_fit<<<1, DT, 0, st>>>(ds, out_dev, (const unsigned long long *)s.shell, s.nshell);
+    k_drop_modes<<<1, ITLBM_N_ANG, 0, st>>>(c_dev, ds, out_dev, s.node);
+    (void)c;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diag_strip(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
+                              int step, int p, int q, bool use_force, itlbm_strip_diag *out_dev,
+                              cudaStream_t st) {
+    StripState *ss = (StripState *)((char *)s.state + sizeof(DropState));
+    const int nb = s.nblocks;
+    cudaMemsetAsync(out_dev, 0, sizeof(itlbm_strip_diag), st);
+    k_strip_s1<<<nb, DT, 0, st>>>(c_dev, cur, p, q, use_force ? 1 : 0, s.part);
+    k_reduce<S_Q, S_NS, S_NM><<<1, DT, 0, st>>>(s.part, nb, ss->a);
+    k_strip_f1<<<1, 1, 0, st>>>(c_dev, ss, p, q, out_dev);
+    k_strip_s2<<<nb, DT, 0, st>>>(c_dev, cur, p, q, ss, s.part);
+    k_reduce<1, 0, 1><<<1, DT, 0, st>>>(s.part, nb, ss->res);
+    k_strip_f2<<<1, 1, 0, st>>>(ss, out_dev);
+    (void)c;
+    (void)step;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fields(const CaseDev *c_dev, const CaseDev &c, int cur, bool use_force,
+                          double *rho_R, double *rho_B, double *ux, double *uy, double *uz,
+                          cudaStream_t st) {
+    const long long n = (long long)c.nx * c.ny;
+    k_fields<<<nblocks_for(n), DT, 0, st>>>(c_dev, cur, use_force ? 1 : 0, rho_R, rho_B, ux, uy, uz);
+    return cudaGetLastError();
+}
+
+}  // namespace itlbm

@@ -1,0 +1,131 @@
+// itlbm_internal.h -- definitions shared by the CUDA translation units of libitlbm.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <type_traits>
+
+#include "../../include/itlbm.h"
+
+namespace itlbm {
+
+constexpr int NV = 19;
+
+// Tile of the fused step: TX x TY interior nodes, one per thread; the phase field is staged with a
+// halo of up to HMAX nodes (1 for P1/P3/F3, 2 for F1/F2).
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int HMAX = 2;
+constexpr int PX = TX + 2 * HMAX;  // staged phase tile width
+constexpr int PY = TY + 2 * HMAX;  // staged phase tile height
+constexpr int QX = TX + 2;         // ring-1 region of the F1/F2 auxiliary fields
+constexpr int QY = TY + 2;
+constexpr int STEP_THREADS = TX * TY;
+
+// D3Q19 velocity set in the order of def_lattice_d3q19 (SimBoltz_Functions/LBM_functions.cpp:366-497)
+__host__ __device__ constexpr int cx(int i) {
+    constexpr int t[NV] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    return t[i];
+}
+__host__ __device__ constexpr int cy(int i) {
+    constexpr int t[NV] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, -1, 1, -1, 1};
+    return t[i];
+}
+__host__ __device__ constexpr int cz(int i) {
+    constexpr int t[NV] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, -1, 1, 1, -1};
+    return t[i];
+}
+__host__ __device__ constexpr int cc(int i) { return cx(i) * cx(i) + cy(i) * cy(i) + cz(i) * cz(i); }
+template <class T>
+__host__ __device__ constexpr T wgt(int i) {
+    return i == 0 ? T(1.) / T(3.) : (i < 7 ? T(1.) / T(18.) : T(1.) / T(36.));
+}
+
+// Compile-time loop: f(std::integral_constant<int, i>) for i in [B, E).
+template <int B, int E, class F>
+__host__ __device__ __forceinline__ void sfor(F &&f) {
+    if constexpr (B < E) {
+        f(std::integral_constant<int, B>{});
+        sfor<B + 1, E>(f);
+    }
+}
+
+// Per-case descriptor read by the step and diagnostic kernels (device memory).
+struct CaseDev {
+    void *buf[2];          // the two state buffers, each 2 x 19 arrays of `stride` elements
+    double *aux;           // 4 arrays of pitch*ny doubles: Fx, Fy, Fz, |grad rho^N| (may be null)
+    long long stride;      // elements per population array (pitch * ny)
+    int nx, ny, pitch;     // box and row pitch (elements)
+    int tiles_x, tiles;    // tiles of this case
+    int tipo;              // ITLBM_OP_*
+    int halo;              // phase-field halo: 1 (P1, P3, F3) or 2 (F1, F2)
+    int prec;              // ITLBM_PREC_*
+    int parity0;           // buffer index holding the state at sub-step k = 0
+    int chunk_len;         // sub-steps to run in this launch sequence (INT_MAX for single cases)
+    int aux_at_end;        // keep aux at sub-step chunk_len - 1
+    double A;              // amplitude (class P)
+    double sigma;          // tension (class F)
+    double beta;           // recolouring factor
+    double inv_tau;        // 1.0 / tau                       (Collision_operators.cpp:18)
+    double src_factor;     // 1. - 1. / (2. * tau)             (LBM_functions.cpp:1648)
+    double B0, B1, B2;     // coef_B of |c|^2 = 0, 1, 2        (Operadores_tensao.cpp:94-109)
+    double kf, bf;         // F3: k = 3 sigma xi / 4, b = 3 sigma / (8 xi) (Operadores_tensao.cpp:240-241)
+    double rho0;           // FP32 shifted storage: reference density of e_i = f_i - w_i rho0
+};
+
+// A tile of the work table: case index and linear tile index within that case.
+struct TileRef {
+    int case_id;
+    int tile;
+};
+
+// ---- kernel launchers (defined in the .cu files) -------------------------------------------
+cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
+                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
+cudaError_t launch_step_f32(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
+                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
+void seam_perturb(int n, double A, double B0, double B1, double B2, const double *g, double *f);
+void seam_source(int n, const double *F, const double *u, double factor, double *S);
+void seam_colisao(int n, const CaseDev &c, bool force, double *fR, double *fB, const double *gm,
+                  const double *F);
+cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
+                        const int *ntiles_dev, int grid, int k, int aux_k, int prec,
+                        cudaStream_t s);
+cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
+                        cudaStream_t s);
+// Export populations to FP64 AoS (reference layout).  which = 0: state of buffer `cur`;
+// which = 1: post-collision of the last step (gathered from buffer `cur`).
+cudaError_t launch_export(const CaseDev *c_dev, int nx, int ny, int cur, int which, double *fR,
+                          double *fB, cudaStream_t s);
+cudaError_t launch_import(const CaseDev *c_dev, int nx, int ny, int cur, const double *fR,
+                          const double *fB, cudaStream_t s);
+
+// Diagnostic scratch (per case, allocated on demand).
+struct DiagScratch {
+    double *node = nullptr;      // per node: rho_R, rho_B, ux, uy, uz, phi (6 arrays of n)
+    double *part = nullptr;      // per-block partial sums
+    long long *shell = nullptr;  // shell histogram (fixed point) and counts
+    double *state = nullptr;     // device-side running state of one diagnostic
+    void *out = nullptr;         // device copy of the output struct
+    int n = 0, nblocks = 0, nshell = 0;
+};
+cudaError_t diag_alloc(DiagScratch &s, int nx, int ny);
+void diag_free(DiagScratch &s);
+cudaError_t launch_diag_drop(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
+                             int step, double v0, double x_ini, double y_ini, bool use_force,
+                             itlbm_drop_diag *out_dev, cudaStream_t st);
+cudaError_t launch_diag_strip(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
+                              int step, int p, int q, bool use_force, itlbm_strip_diag *out_dev,
+                              cudaStream_t st);
+cudaError_t launch_fields(const CaseDev *c_dev, const CaseDev &c, int cur, bool use_force,
+                          double *rho_R, double *rho_B, double *ux, double *uy, double *uz,
+                          cudaStream_t st);
+
+// ---- error reporting -------------------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+}  // namespace itlbm

@@ -1,0 +1,394 @@
+// itlbm_site.cuh -- per-site device physics of the colour-gradient step.
+//
+// Two forms of the same site update:
+//   * collide_f64: the populations f_R, f_B in FP64, with the reference's arithmetic in the
+//     reference's operation order (colisao_comum, Operadores_tensao.cpp:340-373, and the library
+//     functions it calls).  Velocity components equal to zero are skipped in the dot products; with
+//     round-to-nearest that changes no finite result (adding a signed zero to a non-zero partial sum
+//     is exact), and the paired directions c_i, -c_i share one division because negation commutes
+//     with rounding.
+//   * collide_f32: FP32 storage of e_i = f_i - w_i rho0 (the deviation of the total population) and
+//     d_i = f_R,i - f_B,i (the colour difference).  Both are linear in (f_R, f_B), so streaming is
+//     unchanged; rho^N = sum d_i / rho, and the BGK update is applied to the deviation so that the
+//     pressure keeps FP32 relative precision on rho - rho0 instead of on rho.
+#pragma once
+
+#include "itlbm_internal.h"
+
+namespace itlbm {
+
+// ---------------------------------------------------------------------------------------------
+// FP64 plain form
+// ---------------------------------------------------------------------------------------------
+
+// c_i . (a, b, c) summing the non-zero terms in index order (dot_product, LBM_functions.cpp:865-876)
+template <int i, class T>
+__device__ __forceinline__ T cdot(T a, T b, T c3) {
+    T s = T(0);
+    bool first = true;
+    auto add = [&](int ci, T v) {
+        if (ci == 0) return;
+        const T t = ci > 0 ? v : -v;
+        s = first ? t : s + t;
+        first = false;
+    };
+    add(cx(i), a);
+    add(cy(i), b);
+    add(cz(i), c3);
+    return s;
+}
+
+// Guo source term S_i (source, LBM_functions.cpp:1603-1673):
+//   S_i = (1 - 1/2tau) w_i 3 (c_i.F + 3 (c_i.F)(c_i.v) - v.F)
+template <int i>
+__device__ __forceinline__ double guo_source_f64(double factor, double Fx, double Fy, double Fz,
+                                                 double cv, double vF) {
+    const double cF = cdot<i>(Fx, Fy, Fz);
+    return ((factor * wgt<double>(i)) * 3.0) * ((cF + ((3.0 * cF) * cv)) - vF);
+}
+
+// Class-P perturbation (perturbacao, Operadores_tensao.cpp:116-133):
+//   f_i += A |g| (w_i (c_i.g)^2 / |g|^2 - B_i), skipped when |g|^2 <= 1e-60 or A == 0.
+// The 9 direction pairs share (c_i.g)^2; c_i.g is summed in the reference's order.
+__device__ __forceinline__ void perturb_f64(double (&f)[NV], double gmx, double gmy, double gmz,
+                                            double A, double B0, double B1, double B2) {
+    const double mod2 = gmx * gmx + gmy * gmy + gmz * gmz;
+    if (mod2 <= 1.0e-60 || A == 0.0) return;
+    const double amod = A * sqrt(mod2);
+    const double q0 = 0.0;
+    const double qx = ((wgt<double>(1) * gmx) * gmx) / mod2;
+    const double qy = ((wgt<double>(3) * gmy) * gmy) / mod2;
+    const double qz = ((wgt<double>(5) * gmz) * gmz) / mod2;
+    const double s7 = gmx + gmy, s9 = gmx - gmy, s11 = gmx + gmz, s13 = gmx - gmz;
+    const double s16 = gmy + gmz, s17 = -gmy + gmz;
+    const double d7 = ((wgt<double>(7) * s7) * s7) / mod2;
+    const double d9 = ((wgt<double>(9) * s9) * s9) / mod2;
+    const double d11 = ((wgt<double>(11) * s11) * s11) / mod2;
+    const double d13 = ((wgt<double>(13) * s13) * s13) / mod2;
+    const double d16 = ((wgt<double>(16) * s16) * s16) / mod2;
+    const double d17 = ((wgt<double>(17) * s17) * s17) / mod2;
+    const double Q[NV] = {q0, qx,  qx,  qy,  qy,  qz,  qz,  d7,  d7, d9,
+                          d9, d11, d11, d13, d13, d16, d16, d17, d17};
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const double B = cc(i) == 0 ? B0 : (cc(i) == 1 ? B1 : B2);
+        f[i] += amod * (Q[i] - B);
+    });
+}
+
+// Guo forcing, BGK relaxation, class-P perturbation and Latva-Kokko recolouring of one site.
+// On entry fR, fB hold the populations at the top of the step and rho_R, rho_B their sums
+// (density(), LBM_functions.cpp:1582-1590, in index order).  gm is the mediator momentum
+// (= -grad rho^N), F the force (used by class F only).  On exit fR, fB are post-collision.
+template <bool FORCE>
+__device__ __forceinline__ void collide_f64(double (&fR)[NV], double (&fB)[NV], double rho_R,
+                                            double rho_B, double gmx, double gmy, double gmz,
+                                            double Fx, double Fy, double Fz, const CaseDev &c) {
+    const double rho = rho_R + rho_B;
+    if (rho <= 1.0e-30) return;  // Operadores_tensao.cpp:347
+    const double conc_R = rho_R / rho;
+    const double conc_B = 1.0 - conc_R;
+    const double mod = sqrt(gmx * gmx + gmy * gmy + gmz * gmz);
+    double f[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) f[i] = fR[i] + fB[i];
+
+    // coll_BGK (Collision_operators.cpp:8-46) with acc = F / rho (class F) or 0 (class P)
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    if constexpr (FORCE) {
+        ax = Fx / rho;
+        ay = Fy / rho;
+        az = Fz / rho;
+    }
+    // calcula (LBM_functions.cpp:1100-1171)
+    double r = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        r = r + f[i];
+        if constexpr (cx(i) == 1) mx = mx + f[i];
+        if constexpr (cx(i) == -1) mx = mx - f[i];
+        if constexpr (cy(i) == 1) my = my + f[i];
+        if constexpr (cy(i) == -1) my = my - f[i];
+        if constexpr (cz(i) == 1) mz = mz + f[i];
+        if constexpr (cz(i) == -1) mz = mz - f[i];
+    });
+    double vx = 0., vy = 0., vz = 0.;
+    if (r != 0.0) {
+        const double inv = 1.0 / (r);
+        vx = mx * inv;
+        vy = my * inv;
+        vz = mz * inv;
+    }
+    const double vxa = vx + 0.5 * ax, vya = vy + 0.5 * ay, vza = vz + 0.5 * az;
+    // dist_eq (LBM_functions.cpp:890-945) and source (LBM_functions.cpp:1603-1673)
+    const double vquad = (vxa * vxa + vya * vya + vza * vza);
+    const double t_vq = (0.5 * vquad) * 3.0;
+    const double inv_tau = c.inv_tau;
+    double Fxr = 0, Fyr = 0, Fzr = 0, vF = 0, fac3 = 0;
+    if constexpr (FORCE) {
+        Fxr = ax * r;
+        Fyr = ay * r;
+        Fzr = az * r;
+        vF = Fxr * vxa + Fyr * vya + Fzr * vza;
+        fac3 = c.src_factor;
+    }
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const double cv = cdot<i>(vxa, vya, vza);
+        constexpr double w = wgt<double>(i);
+        const double feq = (w * r) * (((1.0 + cv * 3.0) + (((0.5 * cv) * cv) * 3.0) * 3.0) - t_vq);
+        const double op = (feq - f[i]) * inv_tau;
+        if constexpr (FORCE) {
+            f[i] = f[i] + op + guo_source_f64<i>(fac3, Fxr, Fyr, Fzr, cv, vF);
+        } else {
+            f[i] = f[i] + op;
+        }
+    });
+
+    // perturbacao (Operadores_tensao.cpp:116-133), class P only; the sign of g is irrelevant
+    if constexpr (!FORCE) perturb_f64(f, gmx, gmy, gmz, c.A, c.B0, c.B1, c.B2);
+
+    // recolloring (LBM_functions.cpp:1713-1746) with grad = gm, |c_i| = 1 or sqrt(2)
+    const double fator = (c.beta * conc_R) * conc_B;
+    fR[0] = conc_R * f[0];
+    fB[0] = conc_B * f[0];
+    const double den1 = mod * 1.0;
+    const double den2 = mod * sqrt(2.0);
+    const bool nz = (mod != 0.0);
+    const double p1 = gmx, p3 = gmy, p5 = gmz;
+    const double p7 = gmx + gmy, p9 = gmx - gmy, p11 = gmx + gmz, p13 = gmx - gmz;
+    const double p16 = gmy + gmz, p17 = -gmy + gmz;
+    const double k1 = nz ? p1 / den1 : 0.0, k3 = nz ? p3 / den1 : 0.0, k5 = nz ? p5 / den1 : 0.0;
+    const double k7 = nz ? p7 / den2 : 0.0, k9 = nz ? p9 / den2 : 0.0;
+    const double k11 = nz ? p11 / den2 : 0.0, k13 = nz ? p13 / den2 : 0.0;
+    const double k16 = nz ? p16 / den2 : 0.0, k17 = nz ? p17 / den2 : 0.0;
+    // cos_phi_i for i = 1..18 (pairs i, i+1 are opposite directions)
+    const double cosp[NV] = {0.0, k1,  -k1,  k3,   -k3, k5,  -k5, k7,   -k7, k9,
+                             -k9, k11, -k11, k13, -k13, -k16, k16, k17, -k17};
+    sfor<1, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        constexpr double w = wgt<double>(i);
+        const double t = ((fator * w) * rho) * cosp[i];
+        fR[i] = conc_R * f[i] - t;
+        fB[i] = conc_B * f[i] + t;
+    });
+}
+
+// ---------------------------------------------------------------------------------------------
+// FP32 shifted form: e_i = f_i - w_i rho0, d_i = f_R,i - f_B,i
+// ---------------------------------------------------------------------------------------------
+template <bool FORCE>
+__device__ __forceinline__ void collide_f32(float (&e)[NV], float (&d)[NV], float drho, float D,
+                                            float gmx, float gmy, float gmz, float Fx, float Fy,
+                                            float Fz, const CaseDev &c) {
+    const float rho0 = (float)c.rho0;
+    const float rho = rho0 + drho;
+    if (rho <= 1.0e-30f) return;
+    const float inv_rho = 1.0f / rho;
+    const float phi = D * inv_rho;  // rho^N = (rho_R - rho_B) / rho
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if constexpr (FORCE) {
+        ax = Fx * inv_rho;
+        ay = Fy * inv_rho;
+        az = Fz * inv_rho;
+    }
+    float jx = 0.f, jy = 0.f, jz = 0.f;
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if constexpr (cx(i) == 1) jx += e[i];
+        if constexpr (cx(i) == -1) jx -= e[i];
+        if constexpr (cy(i) == 1) jy += e[i];
+        if constexpr (cy(i) == -1) jy -= e[i];
+        if constexpr (cz(i) == 1) jz += e[i];
+        if constexpr (cz(i) == -1) jz -= e[i];
+    });
+    const float vx = jx * inv_rho + 0.5f * ax, vy = jy * inv_rho + 0.5f * ay;
+    const float vz = jz * inv_rho + 0.5f * az;
+    const float usq15 = 1.5f * (vx * vx + vy * vy + vz * vz);
+    const float inv_tau = (float)c.inv_tau;
+    const float Frx = ax * rho, Fry = ay * rho, Frz = az * rho;
+    const float vF = Frx * vx + Fry * vy + Frz * vz;
+    const float fac3 = 3.0f * (float)c.src_factor;
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        constexpr float w = wgt<float>(i);
+        const float cu = (float)cx(i) * vx + (float)cy(i) * vy + (float)cz(i) * vz;
+        // f_eq - w rho0 = w (drho + rho (3 cu + 4.5 cu^2 - 1.5 u^2))
+        const float dfeq = w * (drho + rho * (cu * (3.0f + 4.5f * cu) - usq15));
+        float en = e[i] + (dfeq - e[i]) * inv_tau;
+        if constexpr (FORCE) {
+            const float cF = (float)cx(i) * Frx + (float)cy(i) * Fry + (float)cz(i) * Frz;
+            en += (fac3 * w) * (cF + 3.0f * cF * cu - vF);
+        }
+        e[i] = en;
+    });
+    const float mod2 = gmx * gmx + gmy * gmy + gmz * gmz;
+    const float mod = sqrtf(mod2);
+    if constexpr (!FORCE) {
+        const float A = (float)c.A;
+        if (!(mod2 <= 1.0e-30f || A == 0.0f)) {
+            const float inv2 = 1.0f / mod2;
+            const float amod = A * mod;
+            sfor<0, NV>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                constexpr float w = wgt<float>(i);
+                const float cg = (float)cx(i) * gmx + (float)cy(i) * gmy + (float)cz(i) * gmz;
+                const float B = (float)(cc(i) == 0 ? c.B0 : (cc(i) == 1 ? c.B1 : c.B2));
+                e[i] += amod * (w * cg * cg * inv2 - B);
+            });
+        }
+    }
+    // recolour: d_i = (c_R - c_B) f_i - 2 beta c_R c_B w_i rho cos(phi_i), c_R - c_B = rho^N
+    const float fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
+    const float inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
+    constexpr float rs2 = 0.70710678118654752f;
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        constexpr float w = wgt<float>(i);
+        const float f = w * rho0 + e[i];
+        if constexpr (i == 0) {
+            d[i] = phi * f;
+        } else {
+            const float cg = (float)cx(i) * gmx + (float)cy(i) * gmy + (float)cz(i) * gmz;
+            const float cosp = cg * inv_mod * (cc(i) == 2 ? rs2 : 1.0f);
+            d[i] = phi * f - fat2 * w * cosp;
+        }
+    });
+}
+
+// ---------------------------------------------------------------------------------------------
+// Stencils on a staged phase tile, generic in the real type
+// ---------------------------------------------------------------------------------------------
+
+// Mediator momentum at tile position (px, py): sum_i c_i * (w_i * (phi(x - c_i) * 3)), the
+// momentum() (LBM_functions.cpp:1057-1087) of the mediators after emite_mediadores + propag_site_med
+// (LBM_functions.cpp:1287-1337), accumulated in index order.
+template <class T, int W_>
+__device__ __forceinline__ void mediator_grad(const T (*phi)[W_], int px, int py, T &gx, T &gy,
+                                              T &gz) {
+    T ax = T(0), ay = T(0), az = T(0);
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const T M = wgt<T>(i) * (phi[py - cy(i)][px - cx(i)] * T(3));
+        if constexpr (cx(i) == 1) ax = ax + M;
+        if constexpr (cx(i) == -1) ax = ax - M;
+        if constexpr (cy(i) == 1) ay = ay + M;
+        if constexpr (cy(i) == -1) ay = ay - M;
+        if constexpr (cz(i) == 1) az = az + M;
+        if constexpr (cz(i) == -1) az = az - M;
+    });
+    gx = ax;
+    gy = ay;
+    gz = az;
+}
+
+// Isotropic gradient 3 sum_{i>=1} w_i c_i phi(x + c_i) (Operadores_tensao.cpp:219-235).
+template <class T, int W_>
+__device__ __forceinline__ void iso_grad(const T (*phi)[W_], int px, int py, T &gx, T &gy, T &gz) {
+    T ax = T(0), ay = T(0), az = T(0);
+    sfor<1, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const T ph = wgt<T>(i) * phi[py + cy(i)][px + cx(i)];
+        if constexpr (cx(i) == 1) ax += ph;
+        if constexpr (cx(i) == -1) ax -= ph;
+        if constexpr (cy(i) == 1) ay += ph;
+        if constexpr (cy(i) == -1) ay -= ph;
+        if constexpr (cz(i) == 1) az += ph;
+        if constexpr (cz(i) == -1) az -= ph;
+    });
+    gx = T(3) * ax;
+    gy = T(3) * ay;
+    gz = T(3) * az;
+}
+
+// F3 chemical potential mu = 4 b phi (phi^2 - 1) - k lap phi (Operadores_tensao.cpp:273-287).
+template <class T, int W_>
+__device__ __forceinline__ T chem_pot(const T (*phi)[W_], int px, int py, T kf, T bf) {
+    const T ph = phi[py][px];
+    T lap = T(0);
+    sfor<1, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        lap += wgt<T>(i) * (phi[py + cy(i)][px + cx(i)] - ph);
+    });
+    lap *= T(6);
+    return T(4) * bf * ph * (ph * ph - T(1)) - kf * lap;
+}
+
+// F1 unit normal (Operadores_tensao.cpp:251-258) and F2 stress (:259-272) from the gradient.
+template <class T>
+__device__ __forceinline__ void aux_normal(T gx, T gy, T gz, T *a) {
+    const T m = sqrt(gx * gx + gy * gy + gz * gz);
+    const T inv = (m > T(1.0e-12)) ? T(1) / m : T(0);
+    a[0] = gx * inv;
+    a[1] = gy * inv;
+    a[2] = gz * inv;
+}
+template <class T>
+__device__ __forceinline__ void aux_stress(T gx, T gy, T gz, T sigma, T *a) {
+    const T m = sqrt(gx * gx + gy * gy + gz * gz);
+    const T h = T(0.5) * sigma;
+    const T inv = (m > T(1.0e-30)) ? T(1) / m : T(0);
+    a[0] = h * (m - gx * gx * inv);
+    a[1] = h * (m - gy * gy * inv);
+    a[2] = h * (m - gz * gz * inv);
+    a[3] = -h * gx * gy * inv;
+    a[4] = -h * gx * gz * inv;
+    a[5] = -h * gy * gz * inv;
+}
+
+// F1: kappa = -div_iso(n) (Operadores_tensao.cpp:187-200, :298-305).  aux has AS components.
+template <class T, int AS, int W_>
+__device__ __forceinline__ T curvature(const T (*aux)[W_][AS], int qx, int qy) {
+    T d = T(0);
+    sfor<1, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const T *v = aux[qy + cy(i)][qx + cx(i)];
+        T s = T(0);
+        bool first = true;
+        auto add = [&](int ci, T val) {
+            if (ci == 0) return;
+            const T t = ci > 0 ? val : -val;
+            s = first ? t : s + t;
+            first = false;
+        };
+        add(cx(i), v[0]);
+        add(cy(i), v[1]);
+        add(cz(i), v[2]);
+        d += wgt<T>(i) * s;
+    });
+    return -(T(3) * d);
+}
+
+// F2: F_a = 3 sum_i w_i T_ab(x + c_i) c_ib (Operadores_tensao.cpp:306-324).
+template <class T, int AS, int W_>
+__device__ __forceinline__ void stress_div(const T (*aux)[W_][AS], int qx, int qy, T &Fx, T &Fy,
+                                           T &Fz) {
+    T ax = T(0), ay = T(0), az = T(0);
+    sfor<1, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const T *t = aux[qy + cy(i)][qx + cx(i)];
+        auto dotc = [&](T a, T b, T c3) {
+            T s = T(0);
+            bool first = true;
+            auto add = [&](int ci, T val) {
+                if (ci == 0) return;
+                const T u = ci > 0 ? val : -val;
+                s = first ? u : s + u;
+                first = false;
+            };
+            add(cx(i), a);
+            add(cy(i), b);
+            add(cz(i), c3);
+            return s;
+        };
+        const T w = wgt<T>(i);
+        ax += w * dotc(t[0], t[3], t[4]);
+        ay += w * dotc(t[3], t[1], t[5]);
+        az += w * dotc(t[4], t[5], t[2]);
+    });
+    Fx = T(3) * ax;
+    Fy = T(3) * ay;
+    Fz = T(3) * az;
+}
+
+}  // namespace itlbm

@@ -1,0 +1,201 @@
+// itlbm_state.cu -- initial state and population export / import (compiled with --fmad=false).
+//
+// The initial profile rho^N(r) of a drop (or c_R(s) of a strip) contains exp(); it is evaluated on
+// the host with the same expression as the reference and uploaded, and this kernel finishes the
+// seeding with dist_eq in the reference's operation order, so the FP64 initial state is bit-identical
+// to the reference's.
+#include "itlbm_site.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace itlbm {
+
+namespace {
+
+__device__ __forceinline__ int wrapi(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+__device__ void store_state(const CaseDev &c, int buf, long long off, const double *fR,
+                            const double *fB) {
+    if (c.prec == ITLBM_PREC_F64) {
+        double *d = (double *)c.buf[buf];
+        for (int i = 0; i < NV; i++) {
+            d[(long long)i * c.stride + off] = fR[i];
+            d[(long long)(NV + i) * c.stride + off] = fB[i];
+        }
+    } else {
+        float *d = (float *)c.buf[buf];
+        for (int i = 0; i < NV; i++) {
+            const double wr = wgt<double>(i) * c.rho0;
+            d[(long long)i * c.stride + off] = (float)((fR[i] + fB[i]) - wr);
+            d[(long long)(NV + i) * c.stride + off] = (float)(fR[i] - fB[i]);
+        }
+    }
+}
+
+// dist_eq (LBM_functions.cpp:890-945) of one colour
+__device__ void dist_eq_dev(double *feq, double vx, double vy, double vz, double rho) {
+    const double vquad = (vx * vx + vy * vy + vz * vz);
+    sfor<0, NV>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        const double cv = cdot<i>(vx, vy, vz);
+        feq[i] = wgt<double>(i) * rho *
+                 (1.0 + cv * 3.0 + 0.5 * cv * cv * 3.0 * 3.0 - 0.5 * vquad * 3.0);
+    });
+}
+
+// initial_conditions_drop (Initial_conditions.cpp:37-169) as called at Imm_OPS.cpp:199-202, given
+// phi(x) from the host: rho_tot = rho_B + phi (rho_R - rho_B) + phi * delta_rho (delta_rho = 0),
+// f_R = dist_eq(v0, phi rho_tot), f_B = dist_eq(v0, (1 - phi) rho_tot).
+// The logistic strip of Imm_INCL.cpp:309-334, given c_R(s) for s = (p x + q y) mod N:
+// f_R = w_i c_R, f_B = w_i (1 - c_R).
+__global__ void k_init(const CaseDev *__restrict__ cp, int geometry, const double *__restrict__ prof,
+                       double v0, double rho_Ri, double rho_Bi, int p, int q) {
+    const CaseDev &c = *cp;
+    const long long n = (long long)c.nx * c.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(t % c.nx), y = (int)(t / c.nx);
+        double fR[NV], fB[NV];
+        if (geometry == ITLBM_GEOM_DROP) {
+            const double phi = prof[t];
+            const double rho_tot = rho_Bi + phi * (rho_Ri - rho_Bi) + phi * 0.0;
+            dist_eq_dev(fR, v0, 0., 0., phi * rho_tot);
+            dist_eq_dev(fB, v0, 0., 0., (1.0 - phi) * rho_tot);
+        } else {
+            const int N = c.nx;
+            long long s = ((long long)p * x + (long long)q * y) % N;
+            if (s < 0) s += N;
+            const double cR = prof[s];
+            for (int i = 0; i < NV; i++) {
+                fR[i] = wgt<double>(i) * cR;
+                fB[i] = wgt<double>(i) * (1.0 - cR);
+            }
+        }
+        store_state(c, c.parity0, (long long)y * c.pitch + x, fR, fB);
+    }
+}
+
+// FP64 AoS export (reference layout f[pto*19+i]); which = 1 gathers the post-collision values of
+// the last step, dst(x + c_i, i).
+__global__ void k_export(const CaseDev *__restrict__ cp, int cur, int which, double *__restrict__ oR,
+                         double *__restrict__ oB) {
+    const CaseDev &c = *cp;
+    const long long n = (long long)c.nx * c.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(t % c.nx), y = (int)(t / c.nx);
+        for (int i = 0; i < NV; i++) {
+            int xs = x, ys = y;
+            if (which) {
+                xs = wrapi(x + cx(i), c.nx);
+                ys = wrapi(y + cy(i), c.ny);
+            }
+            const long long off = (long long)ys * c.pitch + xs;
+            double r, b;
+            if (c.prec == ITLBM_PREC_F64) {
+                const double *d = (const double *)c.buf[cur];
+                r = d[(long long)i * c.stride + off];
+                b = d[(long long)(NV + i) * c.stride + off];
+            } else {
+                const float *d = (const float *)c.buf[cur];
+                const double e = d[(long long)i * c.stride + off];
+                const double dd = d[(long long)(NV + i) * c.stride + off];
+                const double f = wgt<double>(i) * c.rho0 + e;
+                r = 0.5 * (f + dd);
+                b = 0.5 * (f - dd);
+            }
+            oR[t * NV + i] = r;
+            oB[t * NV + i] = b;
+        }
+    }
+}
+
+__global__ void k_import(const CaseDev *__restrict__ cp, int cur, const double *__restrict__ iR,
+                         const double *__restrict__ iB) {
+    const CaseDev &c = *cp;
+    const long long n = (long long)c.nx * c.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(t % c.nx), y = (int)(t / c.nx);
+        store_state(c, cur, (long long)y * c.pitch + x, iR + t * NV, iB + t * NV);
+    }
+}
+
+int grid_for(long long n, int threads) {
+    long long g = (n + threads - 1) / threads;
+    if (g > 148LL * 32) g = 148LL * 32;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+// Host side of the initial profile: the expressions of Initial_conditions.cpp:66-86 (drop) and
+// Imm_INCL.cpp:310-324 (strip), evaluated with the host's libm like the reference does.
+cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
+                        cudaStream_t s) {
+    const long long n = (long long)c.nx * c.ny;
+    std::vector<double> prof;
+    if (d.geometry == ITLBM_GEOM_DROP) {
+        const double radius = d.radius > 0.0 ? d.radius : 0.25 * (double)d.nx;
+        const double k_perfil = d.k_profile;
+        const int x0 = c.nx / 2, y0 = c.ny / 2;
+        prof.resize(n);
+        for (int y = 0; y < c.ny; y++)
+            for (int x = 0; x < c.nx; x++) {
+                const double dx = (double)(x - x0), dy = (double)(y - y0), dz = 0.0;
+                const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+                double phi;
+                if (k_perfil > 0.0) {
+                    double arg = k_perfil * (r - radius);
+                    if (arg > 60.0) arg = 60.0;
+                    if (arg < -60.0) arg = -60.0;
+                    phi = 1.0 / (1.0 + std::exp(arg));
+                } else {
+                    phi = (r < radius) ? 1.0 : 0.0;
+                }
+                prof[(size_t)y * c.nx + x] = phi;
+            }
+    } else {
+        const int N = c.nx, p = d.p, q = d.q;
+        const double m = std::sqrt((double)(p * p + q * q));
+        const double k = 2.0 * std::log(9.0) / 3.45;
+        prof.resize(N);
+        for (long long s2 = 0; s2 < N; s2++) {
+            const double dred = (2 * s2 < N) ? std::min((double)s2, 0.5 * N - s2) / m
+                                             : -std::min(s2 - 0.5 * N, (double)(N - s2)) / m;
+            prof[s2] = 1.0 / (1.0 + std::exp(-k * dred));
+        }
+    }
+    double *dprof = nullptr;
+    cudaError_t e = cudaMalloc(&dprof, sizeof(double) * prof.size());
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(dprof, prof.data(), sizeof(double) * prof.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_init<<<grid_for(n, 256), 256, 0, s>>>(c_dev, d.geometry, dprof, d.v0, d.rho_R, d.rho_B,
+                                                d.p, d.q);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(dprof);
+    return e;
+}
+
+cudaError_t launch_export(const CaseDev *c_dev, int nx, int ny, int cur, int which, double *fR,
+                          double *fB, cudaStream_t s) {
+    k_export<<<grid_for((long long)nx * ny, 256), 256, 0, s>>>(c_dev, cur, which, fR, fB);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_import(const CaseDev *c_dev, int nx, int ny, int cur, const double *fR,
+                          const double *fB, cudaStream_t s) {
+    k_import<<<grid_for((long long)nx * ny, 256), 256, 0, s>>>(c_dev, cur, fR, fB);
+    return cudaGetLastError();
+}
+
+}  // namespace itlbm

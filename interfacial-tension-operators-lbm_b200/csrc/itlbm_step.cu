@@ -1,0 +1,258 @@
+// itlbm_step.cu -- the fused time step, the initial state and population export/import.
+//
+// State layout in HBM (per case, per buffer): 2 colours x 19 directions x `stride` elements, one
+// structure-of-arrays plane per (colour, i), rows of `pitch` elements (pitch = nx rounded up to 32).
+//   FP64 plain:  plane (0, i) = f_R,i and (1, i) = f_B,i
+//   FP32 shifted: plane (0, i) = e_i = f_i - w_i rho0 and (1, i) = d_i = f_R,i - f_B,i
+// A buffer holds the populations at the top of a step -- the reference's inif_R / inif_B after the
+// swap (Imm_OPS.cpp:368-371) -- so initial states need no shift.  The step reads buffer `src`,
+// collides every node and pushes each post-collision population to its neighbour x + c_i in buffer
+// `dst`, as propag_site does (SimBoltz_Functions/LBM_functions.cpp:1220-1247).  The post-collision
+// values the diagnostics need are therefore dst(x + c_i, i).
+//
+// One CTA handles a TX x TY tile of one case (the work table says which).  It stages rho^N for the
+// tile plus a halo of 1 (P1, P3, F3) or 2 (F1, F2) nodes in shared memory -- the halo nodes are
+// re-read from L2, where the neighbouring tiles keep them -- then evaluates the mediator gradient,
+// the force of class F on a ring-1 region of auxiliary fields, and collides.  No mediator
+// populations or force fields ever reach HBM.
+#include "itlbm_site.cuh"
+
+#include <climits>
+
+namespace itlbm {
+
+namespace {
+
+__device__ __forceinline__ int wrapi(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+template <class S>
+struct SmemT {
+    S phi[PY][PX];        // rho^N of tile + halo (HMAX), position (px, py) = global (x0-2+px, y0-2+py)
+    S g[QY][QX][3];       // ring-1 gradient (F1, F2)
+    S aux[QY][QX][6];     // ring-1 normal (F1) or stress (F2)
+};
+
+// ---- loads ------------------------------------------------------------------------------------
+// FP64: sums rho_R, rho_B in index order (density(), LBM_functions.cpp:1582-1590) and
+// rho^N = (rho_R - rho_B) / (rho_R + rho_B) as at Imm_OPS.cpp:255-258.
+__device__ __forceinline__ void load_node(const double *__restrict__ src, long long stride,
+                                          long long off, double (&a)[NV], double (&b)[NV],
+                                          double &sa, double &sb) {
+    sa = 0.0;
+    sb = 0.0;
+#pragma unroll
+    for (int i = 0; i < NV; i++) a[i] = __ldg(src + (long long)i * stride + off);
+#pragma unroll
+    for (int i = 0; i < NV; i++) b[i] = __ldg(src + (long long)(NV + i) * stride + off);
+#pragma unroll
+    for (int i = 0; i < NV; i++) sa = sa + a[i];
+#pragma unroll
+    for (int i = 0; i < NV; i++) sb = sb + b[i];
+}
+__device__ __forceinline__ void load_node(const float *__restrict__ src, long long stride,
+                                          long long off, float (&a)[NV], float (&b)[NV], float &sa,
+                                          float &sb) {
+    sa = 0.f;
+    sb = 0.f;
+#pragma unroll
+    for (int i = 0; i < NV; i++) a[i] = __ldg(src + (long long)i * stride + off);
+#pragma unroll
+    for (int i = 0; i < NV; i++) b[i] = __ldg(src + (long long)(NV + i) * stride + off);
+#pragma unroll
+    for (int i = 0; i < NV; i++) sa += a[i];
+#pragma unroll
+    for (int i = 0; i < NV; i++) sb += b[i];
+}
+__device__ __forceinline__ double phase_of(double rR, double rB, const CaseDev &) {
+    return (rR - rB) / (rR + rB);
+}
+__device__ __forceinline__ float phase_of(float drho, float D, const CaseDev &c) {
+    return D / ((float)c.rho0 + drho);
+}
+
+// rho^N of one node, without keeping its populations (halo nodes).
+template <class S>
+__device__ __forceinline__ S phase_at(const S *__restrict__ src, long long stride, long long off,
+                                      const CaseDev &c) {
+    S sa = S(0), sb = S(0);
+#pragma unroll
+    for (int i = 0; i < NV; i++) sa = sa + __ldg(src + (long long)i * stride + off);
+#pragma unroll
+    for (int i = 0; i < NV; i++) sb = sb + __ldg(src + (long long)(NV + i) * stride + off);
+    return phase_of(sa, sb, c);
+}
+
+// ring position r -> staged-tile coordinates (px, py) for a halo of H around the TX x TY interior
+__device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
+    const int W = TX + 2 * H;
+    const int nTop = H * W;
+    if (r < nTop) {
+        py = HMAX - H + r / W;
+        px = HMAX - H + r % W;
+    } else if (r < 2 * nTop) {
+        r -= nTop;
+        py = HMAX + TY + r / W;
+        px = HMAX - H + r % W;
+    } else {
+        r -= 2 * nTop;
+        py = HMAX + r / (2 * H);
+        const int k = r % (2 * H);
+        px = k < H ? HMAX - H + k : HMAX + TX + (k - H);
+    }
+}
+
+template <class S, bool FORCE>
+__device__ __forceinline__ void collide(S (&a)[NV], S (&b)[NV], S sa, S sb, S gx, S gy, S gz,
+                                        S Fx, S Fy, S Fz, const CaseDev &c) {
+    if constexpr (std::is_same<S, double>::value)
+        collide_f64<FORCE>(a, b, sa, sb, gx, gy, gz, Fx, Fy, Fz, c);
+    else
+        collide_f32<FORCE>(a, b, sa, sb, gx, gy, gz, Fx, Fy, Fz, c);
+}
+
+// One tile of one case.
+template <class S>
+__device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int aux_k,
+                                          SmemT<S> &sm) {
+    const int tid = threadIdx.x;
+    const int lx = tid % TX, ly = tid / TX;
+    const int nx = c.nx, ny = c.ny, pitch = c.pitch;
+    const long long stride = c.stride;
+    const int x0 = (tile % c.tiles_x) * TX, y0 = (tile / c.tiles_x) * TY;
+    const int xe = min(x0 + TX, nx), ye = min(y0 + TY, ny);  // end of the valid interior
+    const int H = c.halo;
+    const int cur = (c.parity0 + k) & 1;
+    const S *__restrict__ src = (const S *)c.buf[cur];
+    S *__restrict__ dst = (S *)c.buf[cur ^ 1];
+    const int tipo = c.tipo;
+
+    // ---- phase A: own node (kept in registers) and rho^N of tile + halo -----------------------
+    const int x = x0 + lx, y = y0 + ly;
+    const bool valid = (x < xe) && (y < ye);
+    S a[NV], b[NV], sa = S(0), sb = S(0);
+    if (x < xe + H && y < ye + H) {
+        const int xw = valid ? x : wrapi(x, nx), yw = valid ? y : wrapi(y, ny);
+        load_node(src, stride, (long long)yw * pitch + xw, a, b, sa, sb);
+        sm.phi[ly + HMAX][lx + HMAX] = phase_of(sa, sb, c);
+    }
+    const int nring = (TX + 2 * H) * (TY + 2 * H) - TX * TY;
+    for (int r = tid; r < nring; r += STEP_THREADS) {
+        int px, py;
+        ring_pos(r, H, px, py);
+        const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
+        if (gx < xe + H && gy < ye + H) {
+            const int xw = wrapi(gx, nx), yw = wrapi(gy, ny);
+            sm.phi[py][px] = phase_at(src, stride, (long long)yw * pitch + xw, c);
+        }
+    }
+    __syncthreads();
+
+    // ---- phase B: ring-1 gradient and normal / stress (F1, F2) -------------------------------
+    const bool ring_aux = (tipo == ITLBM_OP_F1 || tipo == ITLBM_OP_F2);
+    if (ring_aux) {
+        for (int q = tid; q < QX * QY; q += STEP_THREADS) {
+            const int qx = q % QX, qy = q / QX;
+            const int gx = x0 - 1 + qx, gy = y0 - 1 + qy;
+            if (gx < xe + 1 && gy < ye + 1) {
+                S g0, g1, g2;
+                iso_grad(sm.phi, qx + 1, qy + 1, g0, g1, g2);
+                sm.g[qy][qx][0] = g0;
+                sm.g[qy][qx][1] = g1;
+                sm.g[qy][qx][2] = g2;
+                if (tipo == ITLBM_OP_F1) aux_normal(g0, g1, g2, sm.aux[qy][qx]);
+                else aux_stress(g0, g1, g2, (S)c.sigma, sm.aux[qy][qx]);
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- phase C: mediator gradient, force, collision, push ----------------------------------
+    if (valid) {
+        const int px = lx + HMAX, py = ly + HMAX;
+        S gmx, gmy, gmz;
+        mediator_grad(sm.phi, px, py, gmx, gmy, gmz);
+        S Fx = S(0), Fy = S(0), Fz = S(0);
+        const bool force = tipo >= ITLBM_OP_F1;
+        if (tipo == ITLBM_OP_F1) {
+            const int qx = lx + 1, qy = ly + 1;
+            const S kappa = curvature<S, 6>(sm.aux, qx, qy);
+            const S hs = (S(0.5) * (S)c.sigma) * kappa;
+            Fx = hs * sm.g[qy][qx][0];
+            Fy = hs * sm.g[qy][qx][1];
+            Fz = hs * sm.g[qy][qx][2];
+        } else if (tipo == ITLBM_OP_F2) {
+            stress_div<S, 6>(sm.aux, lx + 1, ly + 1, Fx, Fy, Fz);
+        } else if (tipo == ITLBM_OP_F3) {
+            S g0, g1, g2;
+            iso_grad(sm.phi, px, py, g0, g1, g2);
+            const S mu = chem_pot(sm.phi, px, py, (S)c.kf, (S)c.bf);
+            Fx = mu * g0;
+            Fy = mu * g1;
+            Fz = mu * g2;
+        }
+        if (force) collide<S, true>(a, b, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c);
+        else collide<S, false>(a, b, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c);
+
+        // push to x + c_i (periodic)
+        const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
+        const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
+        sfor<0, NV>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            const int xd = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
+            const int yd = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
+            const long long o = (long long)yd * pitch + xd;
+            dst[(long long)i * stride + o] = a[i];
+            dst[(long long)(NV + i) * stride + o] = b[i];
+        });
+
+        if (c.aux != nullptr && (k == aux_k || (c.aux_at_end && k == c.chunk_len - 1))) {
+            const long long o = (long long)y * pitch + x;
+            const long long n = stride;
+            c.aux[o] = (double)Fx;
+            c.aux[n + o] = (double)Fy;
+            c.aux[2 * n + o] = (double)Fz;
+            c.aux[3 * n + o] = sqrt((double)gmx * gmx + (double)gmy * gmy + (double)gmz * gmz);
+        }
+    }
+    __syncthreads();
+}
+
+template <class S>
+__global__ void __launch_bounds__(STEP_THREADS) k_step(const CaseDev *__restrict__ cases,
+                                                       const TileRef *__restrict__ tiles,
+                                                       int ntiles, const int *__restrict__ ntiles_dev,
+                                                       int k, int aux_k) {
+    __shared__ SmemT<S> sm;
+    const int nt = ntiles_dev ? *ntiles_dev : ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const TileRef tr = tiles[t];
+        const CaseDev &c = cases[tr.case_id];
+        if (k >= c.chunk_len) continue;
+        step_tile<S>(c, tr.tile, k, aux_k, sm);
+    }
+}
+
+}  // namespace
+
+// This file is compiled twice: with ITLBM_STEP_F64 (and --fmad=false, so that every FP64 operation
+// rounds exactly as the reference's own code compiled with strict IEEE semantics) and without it.
+#ifdef ITLBM_STEP_F64
+cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
+                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s) {
+    if (grid <= 0) return cudaSuccess;
+    k_step<double><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
+    return cudaGetLastError();
+}
+#else
+cudaError_t launch_step_f32(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
+                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s) {
+    if (grid <= 0) return cudaSuccess;
+    k_step<float><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
+    return cudaGetLastError();
+}
+#endif
+
+}  // namespace itlbm

@@ -1,0 +1,282 @@
+"""Parity of the CUDA path with the oracle (which is bit-identical to the reference's own code built
+with strict IEEE semantics, see test_oracle_pin.py).
+
+The FP64 plain path is compared BIT FOR BIT: initial state, populations at the top of each step,
+post-collision populations and the class-F force.  The bar of the north-star (max |df| <= 1e-12
+after 1000 steps) is therefore met with max |df| = 0.  Diagnostics reduce in a different order on
+the device, so they are compared with a relative tolerance of 1e-10 (absolute floor for quantities
+that are zero up to round-off).
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+OPS = [("P1", 1, 0.5, 1.569988, 0.225), ("P3 -0.4", 3, -0.4, 1.569988, 0.225),
+       ("P3 0.5", 3, 0.5, 1.569988, 0.225), ("P3 2", 3, 2.0, 1.569988, 0.225),
+       ("F1", 11, 0.5, 1.569988, 0.1), ("F2", 12, 0.5, 1.569988, 0.1), ("F3", 13, 0.5, 1.569988, 0.1)]
+OP_IDS = [o[0] for o in OPS]
+
+
+def gpu_case(itlbm, nx, ny, tipo, chi, xi, A, tau=1.0, beta=0.8, radius=0.0, kprof=None, v0=0.0,
+             geometry=0, p=1, q=0, prec=0):
+    op = itlbm.make_op(tipo, chi, xi)
+    kp = 2.0 * math.log(9.0) / 3.45 if kprof is None else kprof
+    d = itlbm.desc(nx, ny, op, tau=tau, beta=beta, A_fact=A, radius=radius, k_profile=kp, v0=v0,
+                   geometry=geometry, p=p, q=q, precision=prec)
+    return itlbm.Case(d)
+
+
+def same(a, b):
+    return np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def maxdiff(a, b):
+    return max(np.abs(a[0] - b[0]).max(), np.abs(a[1] - b[1]).max())
+
+
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=OP_IDS)
+@pytest.mark.parametrize("nx,ny,R,v0,kprof,tau", [
+    (37, 29, 8.5, 0.1, None, 0.7),     # partial tiles in x and y, translating
+    (64, 64, 10.0, 0.0, 0.0, 1.0),     # sharp initial step
+    (7, 5, 2.0, 0.0, None, 0.9),       # smaller than one tile: halo wraps several times
+    (33, 9, 4.0, 0.05, None, 0.55),    # one node more than a tile in x
+])
+def test_fp64_bit_exact_drop(gpu, oracle, name, tipo, chi, xi, A, nx, ny, R, v0, kprof, tau):
+    kp = oracle.K_PERFIL if kprof is None else kprof
+    c = gpu_case(gpu, nx, ny, tipo, chi, xi, A, tau=tau, radius=R, kprof=kp, v0=v0)
+    o = oracle.OracleCase(nx, ny, tipo, chi, xi, tau=tau, beta=0.8, A=A).init_drop(radius=R, k_perfil=kp, v0=v0)
+    assert same(c.read_pops(0), o.pops(0)), "initial state"
+    for chunk in (1, 1, 8, 90):
+        c.step(chunk, keep_aux=True)
+        o.step(chunk)
+        assert same(c.read_pops(0), o.pops(0)), f"state after {c.steps_done} steps: {maxdiff(c.read_pops(0), o.pops(0))}"
+        assert same(c.read_pops(1), o.pops(1)), "post-collision"
+    if tipo >= 11:
+        F = c.read_fields(force=True)["force"]
+        assert np.array_equal(F, o.force())
+    c.close()
+
+
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=OP_IDS)
+@pytest.mark.parametrize("N,p,q", [(40, 3, 1), (30, 1, 0), (64, 1, 1), (50, 4, 1)])
+def test_fp64_bit_exact_strip(gpu, oracle, name, tipo, chi, xi, A, N, p, q):
+    c = gpu_case(gpu, N, N, tipo, chi, xi, A, tau=0.7, geometry=1, p=p, q=q)
+    o = oracle.OracleCase(N, N, tipo, chi, xi, tau=0.7, beta=0.8, A=A).init_strip(p, q)
+    assert same(c.read_pops(0), o.pops(0))
+    c.step(60, keep_aux=True)
+    o.step(60)
+    assert same(c.read_pops(1), o.pops(1))
+    g = c.diag_strip(59).as_dict()
+    r = o.diag_strip(59, p, q).as_dict()
+    for k in r:
+        if k in ("qx", "qy", "SFx", "SFy", "d0"):  # sums that cancel to round-off
+            assert abs(g[k] - r[k]) <= 1e-10 * max(1.0, abs(r[k])), k
+        elif isinstance(r[k], float):
+            assert math.isclose(g[k], r[k], rel_tol=1e-10, abs_tol=1e-14), (k, g[k], r[k])
+        else:
+            assert g[k] == r[k], (k, g[k], r[k])
+    c.close()
+
+
+def test_config1_1000_steps(gpu, oracle):
+    """64x64x1, sharp step R = 10, P3 chi = 0.5, A = 0.225, tau = 1, beta = 0.8, 1000 steps."""
+    c = gpu_case(gpu, 64, 64, 3, 0.5, 1.569988, 0.225, tau=1.0, radius=10.0, kprof=0.0)
+    o = oracle.OracleCase(64, 64, 3, 0.5, 1.569988, tau=1.0, beta=0.8, A=0.225).init_drop(radius=10.0, k_perfil=0.0)
+    m0 = [x.sum() for x in c.read_pops(0)]
+    c.step(999)
+    o.step(999)
+    d_g0 = None
+    c.step(1, keep_aux=True)
+    o.step(1)
+    a, b = c.read_pops(0), o.pops(0)
+    assert maxdiff(a, b) == 0.0
+    # total mass of each colour conserved to round-off
+    m1 = [x.sum() for x in a]
+    assert abs(m1[0] - m0[0]) < 1e-10 * m0[0] and abs(m1[1] - m0[1]) < 1e-10 * m0[1]
+    dg, do = c.diag_drop(999), o.diag_drop(999)
+    assert dg.ok and do.ok
+    for k in ("raio", "raio_grad", "p_in", "p_out", "delta_p", "sigma", "massa_R", "massa_B",
+              "u_max", "u_rms", "K_perfil", "r_perfil", "R0", "a2", "a4", "a8"):
+        assert math.isclose(getattr(dg, k), getattr(do, k), rel_tol=1e-10), k
+    c.close()
+
+
+def close_diag(g, r, rel=1e-10):
+    """Compare two drop diagnostics: relative 1e-10, absolute floor where the value is round-off."""
+    floors = {"qx": 1e-10, "qy": 1e-10, "qz": 1e-10, "mean_x": 1e-13, "mean_y": 1e-13, "mean_z": 1e-13,
+              "drop_x": 1e-13, "drop_y": 1e-13, "center_dx": 1e-9, "center_dy": 1e-9, "delta_p": 1e-14,
+              "sigma": 1e-13, "sigma_linha": 1e-13, "a2": 1e-9, "a4": 1e-9, "a8": 1e-9,
+              "sd_in": 1e-7, "sd_out": 1e-7, "res_perfil": 1e-8, "min_f": 1e-16, "u_max": 1e-14,
+              "u_rms": 1e-14, "max_ref": 1e-14, "rms_ref": 1e-14, "max_mean": 1e-14, "rms_mean": 1e-14,
+              "max_lab": 1e-14, "rms_lab": 1e-14, "axis_ratio": 1e-9, "x_unwrapped": 1e-9}
+    bad = {}
+    for k, v in r.items():
+        gv = g[k]
+        if isinstance(v, float):
+            if math.isnan(v) and math.isnan(gv):
+                continue
+            if not (abs(gv - v) <= rel * abs(v) + floors.get(k, 1e-15)):
+                bad[k] = (gv, v)
+        elif gv != v:
+            bad[k] = (gv, v)
+    return bad
+
+
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=OP_IDS)
+@pytest.mark.parametrize("nx,v0", [(48, 0.0), (61, 0.1)])
+def test_drop_diagnostics(gpu, oracle, name, tipo, chi, xi, A, nx, v0):
+    c = gpu_case(gpu, nx, nx, tipo, chi, xi, A, tau=0.8, v0=v0)
+    o = oracle.OracleCase(nx, nx, tipo, chi, xi, tau=0.8, beta=0.8, A=A).init_drop(v0=v0)
+    for step in (0, 200):
+        n = step + 1 - c.steps_done
+        c.step(n, keep_aux=True)
+        o.step(n)
+        g = c.diag_drop(step).as_dict()
+        r = o.diag_drop(step, v0=v0).as_dict()
+        assert g["ok"] == r["ok"] == 1
+        bad = close_diag(g, r)
+        assert not bad, bad
+    c.close()
+
+
+def test_diag_requires_aux_for_class_f(gpu):
+    c = gpu_case(gpu, 32, 32, 12, 0.5, 1.569988, 0.1)
+    with pytest.raises(gpu.ItlbmError) as e:
+        c.diag_drop(0)
+    assert e.value.code == -10  # no step yet
+    c.step(1)
+    with pytest.raises(gpu.ItlbmError) as e:
+        c.diag_drop(0)
+    assert e.value.code == -10  # class F without the force of the last step
+    c.step(1, keep_aux=True)
+    assert c.diag_drop(1).ok
+    c.close()
+
+
+# ---- E0: verifica_operadores on the device ------------------------------------------------------
+@pytest.mark.parametrize("tipo,chi", [(1, 0.5), (3, -0.4), (3, 0.5), (3, 2.0), (3, 7.0)])
+def test_dev_perturbacao(gpu, oracle, tipo, chi):
+    rng = np.random.default_rng(11)
+    n = 200
+    g = rng.normal(size=(n, 3)) * 0.81
+    g[0] = 0.0            # below the 1e-60 guard: untouched
+    f0 = rng.normal(size=(n, 19)) * 0.01
+    op = gpu.make_op(tipo, chi)
+    fd = gpu.dev_perturbacao(op, 0.37, g, f0)
+    fo = np.array([oracle.perturbacao(tipo, chi, 0.37, g[k], f0[k]) for k in range(n)])
+    assert np.array_equal(fd, fo)
+    # moments (verifica_operadores.cpp:187-234) on the device result, unit |g| = 0.81
+    C = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1], [1, 1, 0],
+                  [-1, -1, 0], [1, -1, 0], [-1, 1, 0], [1, 0, 1], [-1, 0, -1], [1, 0, -1], [-1, 0, 1],
+                  [0, -1, -1], [0, 1, 1], [0, -1, 1], [0, 1, -1]], dtype=float)
+    nn = rng.normal(size=(n, 3))
+    nn /= np.linalg.norm(nn, axis=1)[:, None]
+    fd = gpu.dev_perturbacao(op, 0.37, 0.81 * nn, np.zeros((n, 19)))
+    lam = 0.0 if tipo == 1 else 1.0
+    for k in range(n):
+        f = fd[k]
+        assert abs(f.sum()) <= 1e-14 and np.abs(C.T @ f).max() <= 1e-14
+        M2 = (C.T * f) @ C
+        assert np.abs(M2 - 2 / 9 * 0.37 * 0.81 * (np.outer(nn[k], nn[k]) - lam * np.eye(3))).max() <= 1e-14
+
+
+def test_dev_source(gpu, oracle):
+    rng = np.random.default_rng(3)
+    n = 64
+    F = rng.normal(size=(n, 3)) * 1e-3
+    u = rng.normal(size=(n, 3)) * 0.02
+    rho = 1 + 0.01 * rng.normal(size=n)
+    S = gpu.dev_source(F, u, rho, 0.8)
+    So = np.array([oracle.source(F[k], u[k], rho[k], 0.8) for k in range(n)])
+    assert np.array_equal(S, So)
+    S1 = gpu.dev_source([[1.3e-3, -2.1e-3, 0.0]], [[0.02, -0.01, 0.0]], [1.03], 0.8)[0]
+    C = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1], [1, 1, 0],
+                  [-1, -1, 0], [1, -1, 0], [-1, 1, 0], [1, 0, 1], [-1, 0, -1], [1, 0, -1], [-1, 0, 1],
+                  [0, -1, -1], [0, 1, 1], [0, -1, 1], [0, 1, -1]], dtype=float)
+    assert abs(S1.sum()) <= 1e-16
+    M1 = C.T @ S1
+    assert abs(M1[0] - (1 - 0.5 / 0.8) * 1.3e-3) <= 1e-16 and abs(M1[1] + (1 - 0.5 / 0.8) * 2.1e-3) <= 1e-16
+
+
+@pytest.mark.parametrize("tipo", [11, 12, 13])
+@pytest.mark.parametrize("xi", [1.569988, 3.0, 6.0])
+def test_dev_calcula_forca_tanh(gpu, oracle, golden, tipo, xi):
+    """Class-F force of the fused step kernel on the tanh profiles of verifica_operadores.cpp:325-403."""
+    import test_oracle_e0 as e0
+    nx = ny = 256
+    sigma, R = 0.1, 60.0
+    op = gpu.make_op(tipo, 0.5, xi)
+    fR, fB = e0.tanh_fields(nx, ny, xi, False)
+    F = gpu.dev_calcula_forca(op, sigma, nx, ny, fR, fB)
+    assert np.array_equal(F, oracle.calcula_forca(tipo, xi, sigma, nx, ny, fR, fB))
+    F = F.reshape(-1, 3)
+    fmax = (abs(F[:, 0]) + abs(F[:, 1])).max()
+    fR, fB = e0.tanh_fields(nx, ny, xi, True, R)
+    F = gpu.dev_calcula_forca(op, sigma, nx, ny, fR, fB)
+    assert np.array_equal(F, oracle.calcula_forca(tipo, xi, sigma, nx, ny, fR, fB))
+    F = F.reshape(-1, 3)
+    x, y = np.meshgrid(np.arange(nx), np.arange(ny))
+    dx, dy = (x - nx / 2.0).ravel(), (y - ny / 2.0).ravel()
+    r = np.hypot(dx, dy)
+    m = r >= 1e-9
+    soma = (-(F[m, 0] * dx[m] + F[m, 1] * dy[m]) / r[m] / (2 * math.pi * r[m])).sum()
+    tol_p = 0.2 / xi ** 2 if tipo == 13 else 1e-3
+    tol_d = 1.5 * (xi / R) ** 2 + 5e-4 + (0.25 / xi ** 2 if tipo == 13 else 0.0)
+    assert fmax / (sigma / xi) <= tol_p
+    assert abs(soma / (sigma / R) - 1.0) <= tol_d
+
+
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=OP_IDS)
+def test_dev_colisao_comum(gpu, oracle, name, tipo, chi, xi, A):
+    rng = np.random.default_rng(5)
+    n = 100
+    W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+    cR = rng.uniform(0, 1, size=n)
+    fR = W[None, :] * cR[:, None] * (1 + 0.01 * rng.normal(size=(n, 19)))
+    fB = W[None, :] * (1 - cR)[:, None] * (1 + 0.01 * rng.normal(size=(n, 19)))
+    gm = rng.normal(size=(n, 3)) * 0.1
+    gm[1] = 0.0
+    F = rng.normal(size=(n, 3)) * 1e-3
+    op = gpu.make_op(tipo, chi, xi)
+    aR, aB = gpu.dev_colisao_comum(op, 0.8, A, 0.8, fR, fB, gm, F if tipo >= 11 else None)
+    for k in range(n):
+        bR, bB = fR[k].copy(), fB[k].copy()
+        oracle.orc().orc_colisao_comum(tipo, chi, 0.8, A, 0.8, oracle._ptr(bR), oracle._ptr(bB),
+                                       oracle._ptr(np.ascontiguousarray(gm[k])), oracle._ptr(np.ascontiguousarray(F[k])))
+        assert np.array_equal(aR[k], bR) and np.array_equal(aB[k], bB), k
+
+
+# ---- FP32 shifted storage ----------------------------------------------------------------------
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=OP_IDS)
+def test_fp32_tracks_fp64(gpu, name, tipo, chi, xi, A):
+    """FP32 storage of e = f - w rho0 and d = f_R - f_B stays close to the FP64 path."""
+    nx = 80
+    c64 = gpu_case(gpu, nx, nx, tipo, chi, xi, A, tau=0.8, radius=16.0)
+    c32 = gpu_case(gpu, nx, nx, tipo, chi, xi, A, tau=0.8, radius=16.0, prec=1)
+    a0, b0 = c64.read_pops(0), c32.read_pops(0)
+    assert maxdiff(a0, b0) < 1e-7
+    for c in (c64, c32):
+        c.step(1999)
+        c.step(1, keep_aux=True)
+    d64, d32 = c64.diag_drop(1999), c32.diag_drop(1999)
+    assert d32.ok
+    assert abs(d32.delta_p - d64.delta_p) <= 5e-3 * abs(d64.delta_p)
+    assert abs(d32.raio - d64.raio) <= 1e-5 * d64.raio
+    assert abs(d32.massa_R - d64.massa_R) <= 1e-5 * d64.massa_R
+    assert abs(d32.u_max - d64.u_max) <= 0.05 * d64.u_max + 2e-6
+    c64.close()
+    c32.close()
+
+
+def test_invalid_descriptions_are_rejected(itlbm):
+    """Argument checks happen before any device work (no GPU needed, kept here with the case API)."""
+    op = itlbm.make_op(3, 0.5)
+    for kw in ({"nx": 0}, {"tau": 0.0}, {"precision": 7}, {"geometry": 5}):
+        d = itlbm.desc(kw.get("nx", 16), 16, op, tau=kw.get("tau", 1.0), precision=kw.get("precision", 0),
+                       geometry=kw.get("geometry", 0))
+        with pytest.raises(itlbm.ItlbmError) as e:
+            itlbm.Case(d)
+        assert e.value.code == -1

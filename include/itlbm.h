@@ -179,6 +179,58 @@ int  itlbm_case_write_pops(itlbm_case *c, const double *fR, const double *fB);
 int  itlbm_case_read_fields(itlbm_case *c, double *rho_R, double *rho_B, double *ux, double *uy,
                             double *uz, double *force);
 
+/* ---- batches: many cases stepped together ------------------------------------------------- */
+/* The batched form of the loop Imm_OPS.cpp:246-372 / Imm_INCL.cpp:358-442 for many independent
+ * cases, replacing the process pool of rodar_lote.py (rodar_lote.py:231-243, :300-318).  Admitted
+ * cases keep their state on the device; each advance runs a CUDA graph of persistent step launches
+ * over a device-resident tile work table (every case's tiles, FP32 and FP64 cases side by side),
+ * stops every case at its next diagnostic step (every 500 steps and the last, Imm_OPS.cpp:293),
+ * measures it there and retires it at its step count or when it becomes unstable
+ * (Imm_OPS.cpp:346-352). */
+typedef struct itlbm_batch itlbm_batch;
+
+typedef struct itlbm_batch_config {
+    size_t hbm_budget;        /* device bytes the batch may hold; 0 = 90 % of the free memory    */
+    int    max_cases;         /* slots; 0 = 4096                                                  */
+    int    chunk;             /* steps per graph replay; 0 = 500 (PASSOS_DIAG)                    */
+    int    diag_every;        /* diagnostic interval; 0 = 500                                     */
+    int    ctas_per_sm;       /* persistent CTAs per SM; 0 = from the occupancy of the kernels    */
+} itlbm_batch_config;
+
+enum { ITLBM_EV_DIAG = 0, ITLBM_EV_DONE = 1, ITLBM_EV_UNSTABLE = 2 };
+
+typedef struct itlbm_batch_event {
+    long long tag;            /* the caller's tag of the case                                     */
+    int       kind;           /* ITLBM_EV_*                                                        */
+    int       geometry;       /* ITLBM_GEOM_* : which of drop / strip is filled                    */
+    int       step;           /* step index of the diagnostic (DIAG) or steps run (DONE/UNSTABLE) */
+    double    t_submit, t_event;  /* seconds on the batch clock                                  */
+    itlbm_drop_diag  drop;
+    itlbm_strip_diag strip;
+} itlbm_batch_event;
+
+typedef struct itlbm_batch_stats {
+    int       active, pending, finished;
+    long long node_updates;   /* lattice-node updates done so far                                */
+    double    device_ms;      /* device time of the step launches (CUDA events)                  */
+    size_t    hbm_used;       /* bytes of case state held                                         */
+    int       replays;        /* graph replays so far                                              */
+} itlbm_batch_stats;
+
+/* No case memory is allocated until cases are admitted. */
+int  itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out);
+void itlbm_batch_destroy(itlbm_batch *b);
+/* Queues a case of n_steps steps.  It is admitted at the next advance when its state fits the HBM
+ * budget and a slot is free (ITLBM_E_ADMISSION if it can never fit).  `tag` comes back in events. */
+int  itlbm_batch_submit(itlbm_batch *b, const itlbm_case_desc *d, int n_steps, long long tag);
+/* One round: admit, run one graph replay (every active case advances to its next diagnostic step
+ * or by `chunk` steps), run the diagnostics that fell due, retire finished and unstable cases.
+ * Returns the number of events now waiting (>= 0) or an error code. */
+int  itlbm_batch_advance(itlbm_batch *b, void *stream);
+/* Copies up to `max` waiting events (oldest first) and removes them from the queue. */
+int  itlbm_batch_poll(itlbm_batch *b, itlbm_batch_event *ev, int max);
+int  itlbm_batch_stats_get(const itlbm_batch *b, itlbm_batch_stats *out);
+
 /* ---- operator seam on the device (per-site functions of the reference) -------------------- */
 /* Each call copies its host arrays to the device, runs the same device code the step kernel uses,
  * and copies the result back (sync). */

@@ -89,6 +89,25 @@ class StripDiag(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_cases", C.c_int), ("chunk", C.c_int),
+                ("diag_every", C.c_int), ("ctas_per_sm", C.c_int)]
+
+
+EV_DIAG, EV_DONE, EV_UNSTABLE = 0, 1, 2
+
+
+class BatchEvent(C.Structure):
+    _fields_ = [("tag", C.c_longlong), ("kind", C.c_int), ("geometry", C.c_int), ("step", C.c_int),
+                ("t_submit", C.c_double), ("t_event", C.c_double), ("drop", DropDiag), ("strip", StripDiag)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("active", C.c_int), ("pending", C.c_int), ("finished", C.c_int),
+                ("node_updates", C.c_longlong), ("device_ms", C.c_double), ("hbm_used", C.c_size_t),
+                ("replays", C.c_int)]
+
+
 class ItlbmError(RuntimeError):
     def __init__(self, code, what):
         super().__init__(f"{what}: {ERRORS.get(code, code)} ({code})")
@@ -125,6 +144,12 @@ def lib():
         "itlbm_case_read_pops": (C.c_int, [vp, C.c_int, dp, dp]),
         "itlbm_case_write_pops": (C.c_int, [vp, dp, dp]),
         "itlbm_case_read_fields": (C.c_int, [vp, dp, dp, dp, dp, dp, dp]),
+        "itlbm_batch_create": (C.c_int, [P(BatchConfig), P(vp)]),
+        "itlbm_batch_destroy": (None, [vp]),
+        "itlbm_batch_submit": (C.c_int, [vp, P(CaseDesc), C.c_int, C.c_longlong]),
+        "itlbm_batch_advance": (C.c_int, [vp, vp]),
+        "itlbm_batch_poll": (C.c_int, [vp, P(BatchEvent), C.c_int]),
+        "itlbm_batch_stats_get": (C.c_int, [vp, P(BatchStats)]),
         "itlbm_dev_perturbacao": (C.c_int, [P(Operador), C.c_double, C.c_int, dp, dp]),
         "itlbm_dev_source": (C.c_int, [C.c_int, dp, dp, dp, C.c_double, dp]),
         "itlbm_dev_calcula_forca": (C.c_int, [P(Operador), C.c_double, C.c_int, C.c_int, dp, dp, dp]),
@@ -248,6 +273,54 @@ class Case:
         if force:
             out["force"] = F
         return out
+
+
+class Batch:
+    """Many cases stepped together (itlbm_batch_* of include/itlbm.h)."""
+
+    def __init__(self, hbm_budget=0, max_cases=0, chunk=0, diag_every=0, ctas_per_sm=0):
+        cfg = BatchConfig(hbm_budget, max_cases, chunk, diag_every, ctas_per_sm)
+        h = C.c_void_p()
+        check(lib().itlbm_batch_create(C.byref(cfg), C.byref(h)), "itlbm_batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().itlbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, d: CaseDesc, n_steps: int, tag: int):
+        check(lib().itlbm_batch_submit(self._h, C.byref(d), n_steps, tag), "itlbm_batch_submit")
+
+    def advance(self):
+        r = lib().itlbm_batch_advance(self._h, None)
+        if r < 0:
+            check(r, "itlbm_batch_advance")
+        return r
+
+    def poll(self, max_events=4096):
+        buf = (BatchEvent * max_events)()
+        n = lib().itlbm_batch_poll(self._h, buf, max_events)
+        if n < 0:
+            check(n, "itlbm_batch_poll")
+        return [buf[i] for i in range(n)]
+
+    def stats(self) -> BatchStats:
+        st = BatchStats()
+        check(lib().itlbm_batch_stats_get(self._h, C.byref(st)), "itlbm_batch_stats_get")
+        return st
 
 
 def dev_perturbacao(op, A, g, f):

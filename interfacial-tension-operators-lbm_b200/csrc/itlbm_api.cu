@@ -63,6 +63,10 @@ cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntil
                : launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
 }
 
+int step_occupancy(int prec) {
+    return prec == ITLBM_PREC_F64 ? step_occupancy_f64() : step_occupancy_f32();
+}
+
 static bool op_valid(int t) {
     return t == ITLBM_OP_P1 || t == ITLBM_OP_P3 || t == ITLBM_OP_F1 || t == ITLBM_OP_F2 ||
            t == ITLBM_OP_F3;

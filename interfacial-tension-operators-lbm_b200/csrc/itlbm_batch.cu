@@ -1,0 +1,478 @@
+// itlbm_batch.cu -- many cases stepped together (include/itlbm.h, itlbm_batch_*).
+//
+// The reference runs one process per case (rodar_lote.py:231-243, a thread pool of subprocesses at
+// :300-318).  Here every admitted case keeps its double-buffered state on the device and all of them
+// advance together:
+//   * a slot table of per-case descriptors (CaseDev) lives in device memory; each descriptor carries
+//     the case's buffer parity and the number of sub-steps it runs in the current replay;
+//   * a tile work table lists the TX x TY tiles of every active case (one table for FP64 cases, one
+//     for FP32 cases) with its length in device memory;
+//   * one replay is a CUDA graph of `chunk` sub-steps, each one persistent launch per precision whose
+//     CTAs stride over the work table; a case whose chunk is shorter skips its tiles in the remaining
+//     sub-steps.  The graph never changes when cases come and go: only the tables do.
+// Each case stops at its next diagnostic step (every diag_every steps and its last step, as
+// Imm_OPS.cpp:293), is measured there by the same device diagnostics as a single case, and retires at
+// its step count or when the stop rule of Imm_OPS.cpp:346-352 / Imm_INCL.cpp:428-433 fires.
+#include "itlbm_site.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <vector>
+
+namespace itlbm {
+void fill_params(CaseDev &c, const itlbm_operador &op, double tau, double A_fact, double beta,
+                 double rho0);
+}  // namespace itlbm
+
+using namespace itlbm;
+
+namespace {
+
+struct Pending {
+    itlbm_case_desc desc;
+    int n_steps;
+    long long tag;
+    double t_submit;
+};
+
+struct Active {
+    itlbm_case_desc desc{};
+    int n_steps = 0;
+    long long tag = 0;
+    double t_submit = 0;
+    int slot = -1;
+    void *mem = nullptr;
+    double *aux = nullptr;
+    size_t bytes = 0;
+    int next_step = 0;  // index of the next step to run
+    int parity = 0;     // buffer holding the state at next_step
+    int chunk_len = 0;
+    bool diag_at_end = false;
+};
+
+size_t case_bytes(const itlbm_case_desc &d, bool &need_aux) {
+    const long long pitch = (d.nx + 31) / 32 * 32;
+    const long long stride = pitch * d.ny;
+    const size_t elem = d.precision == ITLBM_PREC_F64 ? 8 : 4;
+    need_aux = d.op.tipo >= ITLBM_OP_F1 || d.geometry == ITLBM_GEOM_STRIP;
+    return (size_t)2 * 2 * NV * stride * elem + (need_aux ? (size_t)4 * stride * 8 : 0);
+}
+
+const double U_LIMITE = 0.4;  // Imm_OPS.cpp:45
+
+}  // namespace
+
+struct itlbm_batch {
+    itlbm_batch_config cfg{};
+    int device = 0, sms = 0;
+    cudaStream_t stream = nullptr;
+    std::deque<Pending> pending;
+    std::vector<Active *> slots;
+    std::vector<int> free_slots;
+    std::vector<CaseDev> h_cases;
+    CaseDev *d_cases = nullptr;
+    TileRef *d_tiles[2] = {nullptr, nullptr};  // [0] FP64 cases, [1] FP32 cases
+    int tiles_cap[2] = {0, 0};
+    int *d_ntiles = nullptr;
+    bool tables_dirty = true;
+    int grid[2] = {0, 0};
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DiagScratch diag;
+    int diag_nx = 0, diag_ny = 0;
+    itlbm_drop_diag *d_drop = nullptr;
+    itlbm_strip_diag *d_strip = nullptr;
+    std::vector<itlbm_drop_diag> h_drop;
+    std::vector<itlbm_strip_diag> h_strip;
+    std::deque<itlbm_batch_event> events;
+    std::chrono::steady_clock::time_point t0;
+    size_t hbm_used = 0;
+    long long node_updates = 0;
+    double device_ms = 0;
+    int replays = 0, finished = 0;
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+int upload_tables(itlbm_batch *b) {
+    std::vector<TileRef> t[2];
+    for (Active *a : b->slots) {
+        if (!a) continue;
+        const CaseDev &c = b->h_cases[a->slot];
+        const int p = a->desc.precision == ITLBM_PREC_F64 ? 0 : 1;
+        for (int k = 0; k < c.tiles; k++) t[p].push_back(TileRef{a->slot, k});
+    }
+    int n[2];
+    for (int p = 0; p < 2; p++) {
+        n[p] = (int)t[p].size();
+        if (n[p] > b->tiles_cap[p]) {
+            if (b->d_tiles[p]) cudaFree(b->d_tiles[p]);
+            b->tiles_cap[p] = std::max(n[p], 2 * b->tiles_cap[p]);
+            cudaError_t e = cudaMalloc(&b->d_tiles[p], sizeof(TileRef) * b->tiles_cap[p]);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(work table)");
+        }
+        if (n[p]) {
+            cudaError_t e = cudaMemcpyAsync(b->d_tiles[p], t[p].data(), sizeof(TileRef) * n[p],
+                                            cudaMemcpyHostToDevice, b->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "work table upload");
+        }
+    }
+    // the graph reads the table pointers it was captured with: keep them, or re-capture
+    cudaError_t e = cudaMemcpyAsync(b->d_ntiles, n, sizeof(int) * 2, cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "work table length");
+    return cudaStreamSynchronize(b->stream) == cudaSuccess ? ITLBM_OK : cuda_fail(cudaGetLastError(), "sync");
+}
+
+int capture_graph(itlbm_batch *b) {
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(e, "begin capture");
+    for (int k = 0; k < b->cfg.chunk; k++) {
+        launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, b->stream);
+        launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->stream);
+    }
+    e = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess) return cuda_fail(e, "end capture");
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "graph instantiate");
+}
+
+void retire(itlbm_batch *b, Active *a) {
+    cudaFree(a->mem);
+    if (a->aux) cudaFree(a->aux);
+    b->hbm_used -= a->bytes;
+    b->slots[a->slot] = nullptr;
+    b->free_slots.push_back(a->slot);
+    b->h_cases[a->slot] = CaseDev{};
+    b->tables_dirty = true;
+    b->finished++;
+    delete a;
+}
+
+int admit(itlbm_batch *b) {
+    while (!b->pending.empty() && !b->free_slots.empty()) {
+        const Pending &p = b->pending.front();
+        bool need_aux;
+        const size_t bytes = case_bytes(p.desc, need_aux);
+        if (b->hbm_used + bytes > b->cfg.hbm_budget) break;  // first in, first admitted
+        Active *a = new Active();
+        a->desc = p.desc;
+        a->n_steps = p.n_steps;
+        a->tag = p.tag;
+        a->t_submit = p.t_submit;
+        a->bytes = bytes;
+        const itlbm_case_desc &d = p.desc;
+        CaseDev h{};
+        h.nx = d.nx;
+        h.ny = d.ny;
+        h.pitch = (d.nx + 31) / 32 * 32;
+        h.stride = (long long)h.pitch * d.ny;
+        h.tiles_x = (d.nx + TX - 1) / TX;
+        h.tiles = h.tiles_x * ((d.ny + TY - 1) / TY);
+        h.prec = d.precision;
+        fill_params(h, d.op, d.tau, d.A_fact, d.beta, d.rho_B > 0 ? d.rho_B : 1.0);
+        const size_t elem = d.precision == ITLBM_PREC_F64 ? 8 : 4;
+        const size_t per_buf = (size_t)2 * NV * h.stride * elem;
+        cudaError_t e = cudaMalloc(&a->mem, 2 * per_buf);
+        if (e == cudaSuccess && need_aux) e = cudaMalloc(&a->aux, sizeof(double) * 4 * (size_t)h.stride);
+        if (e != cudaSuccess) {
+            if (a->mem) cudaFree(a->mem);
+            delete a;
+            cudaGetLastError();
+            return ITLBM_OK;  // the device is fuller than the budget says: try again next round
+        }
+        h.buf[0] = a->mem;
+        h.buf[1] = (char *)a->mem + per_buf;
+        h.aux = a->aux;
+        h.parity0 = 0;
+        h.chunk_len = 0;
+        const int slot = b->free_slots.back();
+        b->free_slots.pop_back();
+        a->slot = slot;
+        b->slots[slot] = a;
+        b->h_cases[slot] = h;
+        e = cudaMemcpy(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = launch_init(h, b->d_cases + slot, d, b->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "admission");
+        b->hbm_used += bytes;
+        b->tables_dirty = true;
+        b->pending.pop_front();
+    }
+    return ITLBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
+    if (!out) return fail(ITLBM_E_ARG, "NULL argument");
+    *out = nullptr;
+    itlbm_batch *b = new itlbm_batch();
+    if (cfg) b->cfg = *cfg;
+    if (b->cfg.max_cases <= 0) b->cfg.max_cases = 4096;
+    if (b->cfg.chunk <= 0) b->cfg.chunk = 500;
+    if (b->cfg.diag_every <= 0) b->cfg.diag_every = 500;
+    cudaError_t e = cudaGetDevice(&b->device);
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "cudaGetDevice");
+    }
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (b->cfg.hbm_budget == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        b->cfg.hbm_budget = (size_t)(0.9 * (double)fr);
+    }
+    for (int p = 0; p < 2; p++) {
+        const int occ = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm : step_occupancy(p == 0 ? ITLBM_PREC_F64 : ITLBM_PREC_F32);
+        b->grid[p] = std::max(1, occ) * b->sms;
+    }
+    const int M = b->cfg.max_cases;
+    b->slots.assign(M, nullptr);
+    for (int s = M - 1; s >= 0; s--) b->free_slots.push_back(s);
+    b->h_cases.assign(M, CaseDev{});
+    b->h_drop.resize(M);
+    b->h_strip.resize(M);
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_cases, sizeof(CaseDev) * M)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_ntiles, sizeof(int) * 2)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_drop, sizeof(itlbm_drop_diag) * M)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_strip, sizeof(itlbm_strip_diag) * M)) != cudaSuccess) {
+        itlbm_batch_destroy(b);
+        return cuda_fail(e, "batch allocation");
+    }
+    cudaMemset(b->d_cases, 0, sizeof(CaseDev) * M);
+    cudaMemset(b->d_ntiles, 0, sizeof(int) * 2);
+    // work tables with room for a first batch, so the graph can be captured with their addresses
+    for (int p = 0; p < 2; p++) {
+        b->tiles_cap[p] = 1 << 16;
+        if ((e = cudaMalloc(&b->d_tiles[p], sizeof(TileRef) * b->tiles_cap[p])) != cudaSuccess) {
+            itlbm_batch_destroy(b);
+            return cuda_fail(e, "work table");
+        }
+    }
+    cudaEventCreate(&b->ev0);
+    cudaEventCreate(&b->ev1);
+    b->t0 = std::chrono::steady_clock::now();
+    int r = capture_graph(b);
+    if (r) {
+        itlbm_batch_destroy(b);
+        return r;
+    }
+    *out = b;
+    return ITLBM_OK;
+}
+
+void itlbm_batch_destroy(itlbm_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (Active *a : b->slots)
+        if (a) {
+            cudaFree(a->mem);
+            if (a->aux) cudaFree(a->aux);
+            delete a;
+        }
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->d_cases) cudaFree(b->d_cases);
+    for (int p = 0; p < 2; p++)
+        if (b->d_tiles[p]) cudaFree(b->d_tiles[p]);
+    if (b->d_ntiles) cudaFree(b->d_ntiles);
+    if (b->d_drop) cudaFree(b->d_drop);
+    if (b->d_strip) cudaFree(b->d_strip);
+    diag_free(b->diag);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int itlbm_batch_submit(itlbm_batch *b, const itlbm_case_desc *d, int n_steps, long long tag) {
+    if (!b || !d || n_steps < 1) return fail(ITLBM_E_ARG, "bad argument");
+    if (d->nx < 1 || d->ny < 1 || !(d->tau > 0.0) ||
+        (d->precision != ITLBM_PREC_F64 && d->precision != ITLBM_PREC_F32) ||
+        (d->geometry != ITLBM_GEOM_DROP && d->geometry != ITLBM_GEOM_STRIP) ||
+        (d->geometry == ITLBM_GEOM_STRIP && (d->nx != d->ny || (d->p == 0 && d->q == 0))))
+        return fail(ITLBM_E_ARG, "invalid case description");
+    bool need_aux;
+    if (case_bytes(*d, need_aux) > b->cfg.hbm_budget)
+        return fail(ITLBM_E_ADMISSION, "case larger than the batch's HBM budget");
+    b->pending.push_back(Pending{*d, n_steps, tag, b->now()});
+    return ITLBM_OK;
+}
+
+int itlbm_batch_advance(itlbm_batch *b, void *stream) {
+    (void)stream;  // the batch runs on its own stream (graphs cannot be captured on the legacy one)
+    if (!b) return fail(ITLBM_E_ARG, "NULL batch");
+    cudaSetDevice(b->device);
+    int r = admit(b);
+    if (r) return r;
+    // plan: every case runs to its next diagnostic step, at most `chunk` steps
+    const int de = b->cfg.diag_every;
+    int K = 0;
+    long long updates = 0;
+    for (Active *a : b->slots) {
+        if (!a) continue;
+        int d = ((a->next_step + de - 1) / de) * de;  // next multiple of diag_every >= next_step
+        if (d > a->n_steps - 1) d = a->n_steps - 1;
+        a->chunk_len = std::min(d - a->next_step + 1, b->cfg.chunk);
+        a->diag_at_end = (a->next_step + a->chunk_len - 1 == d);
+        CaseDev &h = b->h_cases[a->slot];
+        h.parity0 = a->parity;
+        h.chunk_len = a->chunk_len;
+        h.aux_at_end = (a->diag_at_end && a->aux) ? 1 : 0;
+        K = std::max(K, a->chunk_len);
+        updates += (long long)a->chunk_len * a->desc.nx * a->desc.ny;
+    }
+    if (K == 0) return (int)b->events.size();
+    cudaError_t e = cudaMemcpyAsync(b->d_cases, b->h_cases.data(), sizeof(CaseDev) * b->h_cases.size(),
+                                    cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "case table upload");
+    if (b->tables_dirty) {
+        TileRef *old0 = b->d_tiles[0], *old1 = b->d_tiles[1];
+        r = upload_tables(b);
+        if (r) return r;
+        if (old0 != b->d_tiles[0] || old1 != b->d_tiles[1]) {
+            r = capture_graph(b);
+            if (r) return r;
+        }
+        b->tables_dirty = false;
+    }
+    cudaEventRecord(b->ev0, b->stream);
+    if (K == b->cfg.chunk) {
+        e = cudaGraphLaunch(b->graph, b->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "graph launch");
+    } else {
+        for (int k = 0; k < K; k++) {
+            launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, b->stream);
+            launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->stream);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "step launches");
+    }
+    cudaEventRecord(b->ev1, b->stream);
+    b->replays++;
+    b->node_updates += updates;
+    // diagnostics that fell due
+    std::vector<Active *> measured;
+    for (Active *a : b->slots) {
+        if (!a || !a->diag_at_end) continue;
+        if (a->desc.nx > b->diag_nx || a->desc.ny > b->diag_ny) {
+            // one scratch for every case, sized by the largest box seen (diagnostics run in turn)
+            cudaStreamSynchronize(b->stream);
+            b->diag_nx = std::max(b->diag_nx, a->desc.nx);
+            b->diag_ny = std::max(b->diag_ny, a->desc.ny);
+            e = diag_alloc(b->diag, b->diag_nx, b->diag_ny);
+            if (e != cudaSuccess) return cuda_fail(e, "diagnostic scratch");
+        }
+        // the scratch is sized for the largest case; the kernels only use the first n entries, but
+        // the shell histogram length depends on the box diagonal, so re-derive it per case
+        DiagScratch s = b->diag;
+        s.n = a->desc.nx * a->desc.ny;
+        s.nshell = (int)(sqrt((double)(a->desc.nx * a->desc.nx + a->desc.ny * a->desc.ny + 1)) / 0.5) + 2;
+        {
+            long long nb = ((long long)s.n + 255) / 256;
+            s.nblocks = (int)std::max(1LL, std::min(nb, (long long)148 * 8));
+        }
+        const int step = a->next_step + a->chunk_len - 1;
+        const int cur = a->parity ^ (a->chunk_len & 1);
+        const CaseDev &h = b->h_cases[a->slot];
+        if (a->desc.geometry == ITLBM_GEOM_DROP)
+            e = launch_diag_drop(b->d_cases + a->slot, h, s, cur, step, a->desc.v0, a->desc.nx / 2,
+                                 a->desc.ny / 2, a->desc.op.tipo >= ITLBM_OP_F1, b->d_drop + a->slot, b->stream);
+        else
+            e = launch_diag_strip(b->d_cases + a->slot, h, s, cur, step, a->desc.p, a->desc.q,
+                                  a->desc.op.tipo >= ITLBM_OP_F1, b->d_strip + a->slot, b->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "diagnostics");
+        measured.push_back(a);
+    }
+    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "replay");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->device_ms += ms;
+    if (!measured.empty()) {
+        int lo = INT_MAX, hi = -1;
+        for (Active *a : measured) {
+            lo = std::min(lo, a->slot);
+            hi = std::max(hi, a->slot);
+        }
+        e = cudaMemcpy(b->h_drop.data() + lo, b->d_drop + lo, sizeof(itlbm_drop_diag) * (hi - lo + 1), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->h_strip.data() + lo, b->d_strip + lo, sizeof(itlbm_strip_diag) * (hi - lo + 1), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "diagnostic copy");
+    }
+    const double t = b->now();
+    std::vector<Active *> gone;
+    for (Active *a : measured) {
+        itlbm_batch_event ev{};
+        ev.tag = a->tag;
+        ev.kind = ITLBM_EV_DIAG;
+        ev.geometry = a->desc.geometry;
+        ev.step = a->next_step + a->chunk_len - 1;
+        ev.t_submit = a->t_submit;
+        ev.t_event = t;
+        bool unstable;
+        if (a->desc.geometry == ITLBM_GEOM_DROP) {
+            ev.drop = b->h_drop[a->slot];
+            ev.drop.step = ev.step;
+            unstable = !ev.drop.ok || ev.drop.n_ruim > 0 || ev.drop.u_max > U_LIMITE;
+        } else {
+            ev.strip = b->h_strip[a->slot];
+            ev.strip.step = ev.step;
+            unstable = !ev.strip.ok || ev.strip.u_max > U_LIMITE;
+        }
+        b->events.push_back(ev);
+        if (unstable || ev.step == a->n_steps - 1) {
+            itlbm_batch_event fin = ev;
+            fin.kind = unstable ? ITLBM_EV_UNSTABLE : ITLBM_EV_DONE;
+            fin.step = unstable ? ev.step : a->n_steps;
+            b->events.push_back(fin);
+            gone.push_back(a);
+        }
+    }
+    for (Active *a : b->slots) {
+        if (!a) continue;
+        a->next_step += a->chunk_len;
+        a->parity ^= (a->chunk_len & 1);
+    }
+    for (Active *a : gone) retire(b, a);
+    return (int)b->events.size();
+}
+
+int itlbm_batch_poll(itlbm_batch *b, itlbm_batch_event *ev, int max) {
+    if (!b || (max > 0 && !ev)) return fail(ITLBM_E_ARG, "bad argument");
+    int n = 0;
+    while (n < max && !b->events.empty()) {
+        ev[n++] = b->events.front();
+        b->events.pop_front();
+    }
+    return n;
+}
+
+int itlbm_batch_stats_get(const itlbm_batch *b, itlbm_batch_stats *out) {
+    if (!b || !out) return fail(ITLBM_E_ARG, "bad argument");
+    out->active = 0;
+    for (Active *a : b->slots) out->active += a ? 1 : 0;
+    out->pending = (int)b->pending.size();
+    out->finished = b->finished;
+    out->node_updates = b->node_updates;
+    out->device_ms = b->device_ms;
+    out->hbm_used = b->hbm_used;
+    out->replays = b->replays;
+    return ITLBM_OK;
+}
+
+}  // extern "C"

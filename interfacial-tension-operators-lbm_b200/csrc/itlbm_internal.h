@@ -86,6 +86,9 @@ cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int 
                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
 cudaError_t launch_step_f32(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
+int step_occupancy_f64();
+int step_occupancy_f32();
+int step_occupancy(int prec);
 void seam_perturb(int n, double A, double B0, double B1, double B2, const double *g, double *f);
 void seam_source(int n, const double *F, const double *u, double factor, double *S);
 void seam_colisao(int n, const CaseDev &c, bool force, double *fR, double *fB, const double *gm,

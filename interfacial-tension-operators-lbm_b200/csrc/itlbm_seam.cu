@@ -31,15 +31,13 @@ template <bool FORCE>
 __global__ void k_colisao(int n, CaseDev c, double *fR, double *fB, const double *gm, const double *F) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    double a[NV], b[NV], sa = 0.0, sb = 0.0;
+    double a[NV], b[NV];
     for (int i = 0; i < NV; i++) {
         a[i] = fR[(size_t)k * NV + i];
         b[i] = fB[(size_t)k * NV + i];
     }
-    for (int i = 0; i < NV; i++) sa = sa + a[i];
-    for (int i = 0; i < NV; i++) sb = sb + b[i];
     const double F0 = FORCE ? F[3 * k] : 0.0, F1 = FORCE ? F[3 * k + 1] : 0.0, F2 = FORCE ? F[3 * k + 2] : 0.0;
-    collide_f64<FORCE>(a, b, sa, sb, gm[3 * k], gm[3 * k + 1], gm[3 * k + 2], F0, F1, F2, c);
+    colisao_site_f64<FORCE>(a, b, gm[3 * k], gm[3 * k + 1], gm[3 * k + 2], F0, F1, F2, c);
     for (int i = 0; i < NV; i++) {
         fR[(size_t)k * NV + i] = a[i];
         fB[(size_t)k * NV + i] = b[i];

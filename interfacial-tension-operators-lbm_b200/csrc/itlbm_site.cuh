@@ -76,22 +76,62 @@ __device__ __forceinline__ void perturb_f64(double (&f)[NV], double gmx, double 
     });
 }
 
-// Guo forcing, BGK relaxation, class-P perturbation and Latva-Kokko recolouring of one site.
-// On entry fR, fB hold the populations at the top of the step and rho_R, rho_B their sums
-// (density(), LBM_functions.cpp:1582-1590, in index order).  gm is the mediator momentum
-// (= -grad rho^N), F the force (used by class F only).  On exit fR, fB are post-collision.
+// Result of the collision of one site: the recolouring split of the post-collision total f_i
+// (recolloring, LBM_functions.cpp:1713-1746):
+//   f_R,0 = c_R f_0, f_B,0 = c_B f_0; for i >= 1: f_R,i = c_R f_i - t_i, f_B,i = c_B f_i + t_i with
+//   t_i = ((beta c_R c_B) w_i rho) cos(phi_i), cos(phi_i) = (c_i . g) / (|g| |c_i|).
+struct Recolour64 {
+    double cR, cB, frho;   // frho = (beta c_R c_B)... times rho: t_i = (frho_w_i) cos_i
+    double fator, rho;
+    double k[9];           // cos(phi) of the directions 1, 3, 5, 7, 9, 11, 13, 16, 17
+    bool skip;             // rho <= 1e-30: the reference leaves the site unchanged
+};
+
+// cos(phi_i) for i = 0..18 from the 9 independent values (pairs i, i+1 are opposite directions)
+__device__ __forceinline__ double cos_of(const Recolour64 &r, int i) {
+    switch (i) {
+        case 1: return r.k[0];  case 2: return -r.k[0];
+        case 3: return r.k[1];  case 4: return -r.k[1];
+        case 5: return r.k[2];  case 6: return -r.k[2];
+        case 7: return r.k[3];  case 8: return -r.k[3];
+        case 9: return r.k[4];  case 10: return -r.k[4];
+        case 11: return r.k[5]; case 12: return -r.k[5];
+        case 13: return r.k[6]; case 14: return -r.k[6];
+        case 15: return -r.k[7]; case 16: return r.k[7];
+        case 17: return r.k[8]; case 18: return -r.k[8];
+        default: return 0.0;
+    }
+}
+
+// Post-collision colour populations of direction i from the collided total f_i.
+template <int i>
+__device__ __forceinline__ void split64(const Recolour64 &r, double fi, double &fR, double &fB) {
+    if constexpr (i == 0) {
+        fR = r.cR * fi;
+        fB = r.cB * fi;
+    } else {
+        constexpr double w = wgt<double>(i);
+        const double t = ((r.fator * w) * r.rho) * cos_of(r, i);
+        fR = r.cR * fi - t;
+        fB = r.cB * fi + t;
+    }
+}
+
+// Guo forcing, BGK relaxation and class-P perturbation of one site (colisao_comum,
+// Operadores_tensao.cpp:340-373, and the library functions it calls).  On entry f holds
+// f_i = f_R,i + f_B,i (Operadores_tensao.cpp:360) and rho_R, rho_B the colour sums (density(),
+// LBM_functions.cpp:1582-1590, index order).  gm is the mediator momentum (= -grad rho^N), F the force
+// (class F only).  On exit f is the post-BGK total and r holds the recolouring split.
 template <bool FORCE>
-__device__ __forceinline__ void collide_f64(double (&fR)[NV], double (&fB)[NV], double rho_R,
-                                            double rho_B, double gmx, double gmy, double gmz,
-                                            double Fx, double Fy, double Fz, const CaseDev &c) {
+__device__ __forceinline__ void collide_f64(double (&f)[NV], double rho_R, double rho_B, double gmx,
+                                            double gmy, double gmz, double Fx, double Fy, double Fz,
+                                            const CaseDev &c, Recolour64 &rc) {
     const double rho = rho_R + rho_B;
-    if (rho <= 1.0e-30) return;  // Operadores_tensao.cpp:347
+    rc.skip = !(rho > 1.0e-30);  // Operadores_tensao.cpp:347 (rho <= 1e-30: return)
+    if (rc.skip) return;
     const double conc_R = rho_R / rho;
     const double conc_B = 1.0 - conc_R;
     const double mod = sqrt(gmx * gmx + gmy * gmy + gmz * gmz);
-    double f[NV];
-#pragma unroll
-    for (int i = 0; i < NV; i++) f[i] = fR[i] + fB[i];
 
     // coll_BGK (Collision_operators.cpp:8-46) with acc = F / rho (class F) or 0 (class P)
     double ax = 0.0, ay = 0.0, az = 0.0;
@@ -149,41 +189,78 @@ __device__ __forceinline__ void collide_f64(double (&fR)[NV], double (&fB)[NV], 
     if constexpr (!FORCE) perturb_f64(f, gmx, gmy, gmz, c.A, c.B0, c.B1, c.B2);
 
     // recolloring (LBM_functions.cpp:1713-1746) with grad = gm, |c_i| = 1 or sqrt(2)
-    const double fator = (c.beta * conc_R) * conc_B;
-    fR[0] = conc_R * f[0];
-    fB[0] = conc_B * f[0];
+    rc.cR = conc_R;
+    rc.cB = conc_B;
+    rc.rho = rho;
+    rc.fator = (c.beta * conc_R) * conc_B;
     const double den1 = mod * 1.0;
     const double den2 = mod * sqrt(2.0);
     const bool nz = (mod != 0.0);
-    const double p1 = gmx, p3 = gmy, p5 = gmz;
-    const double p7 = gmx + gmy, p9 = gmx - gmy, p11 = gmx + gmz, p13 = gmx - gmz;
-    const double p16 = gmy + gmz, p17 = -gmy + gmz;
-    const double k1 = nz ? p1 / den1 : 0.0, k3 = nz ? p3 / den1 : 0.0, k5 = nz ? p5 / den1 : 0.0;
-    const double k7 = nz ? p7 / den2 : 0.0, k9 = nz ? p9 / den2 : 0.0;
-    const double k11 = nz ? p11 / den2 : 0.0, k13 = nz ? p13 / den2 : 0.0;
-    const double k16 = nz ? p16 / den2 : 0.0, k17 = nz ? p17 / den2 : 0.0;
-    // cos_phi_i for i = 1..18 (pairs i, i+1 are opposite directions)
-    const double cosp[NV] = {0.0, k1,  -k1,  k3,   -k3, k5,  -k5, k7,   -k7, k9,
-                             -k9, k11, -k11, k13, -k13, -k16, k16, k17, -k17};
-    sfor<1, NV>([&](auto I) {
+    rc.k[0] = nz ? gmx / den1 : 0.0;
+    rc.k[1] = nz ? gmy / den1 : 0.0;
+    rc.k[2] = nz ? gmz / den1 : 0.0;
+    rc.k[3] = nz ? (gmx + gmy) / den2 : 0.0;
+    rc.k[4] = nz ? (gmx - gmy) / den2 : 0.0;
+    rc.k[5] = nz ? (gmx + gmz) / den2 : 0.0;
+    rc.k[6] = nz ? (gmx - gmz) / den2 : 0.0;
+    rc.k[7] = nz ? (gmy + gmz) / den2 : 0.0;
+    rc.k[8] = nz ? (-gmy + gmz) / den2 : 0.0;
+}
+
+// The whole site update on arrays, for the per-site seam entry points.
+template <bool FORCE>
+__device__ __forceinline__ void colisao_site_f64(double (&fR)[NV], double (&fB)[NV], double gmx,
+                                                 double gmy, double gmz, double Fx, double Fy,
+                                                 double Fz, const CaseDev &c) {
+    double f[NV], sa = 0.0, sb = 0.0;
+#pragma unroll
+    for (int i = 0; i < NV; i++) sa = sa + fR[i];
+#pragma unroll
+    for (int i = 0; i < NV; i++) sb = sb + fB[i];
+#pragma unroll
+    for (int i = 0; i < NV; i++) f[i] = fR[i] + fB[i];
+    Recolour64 rc;
+    collide_f64<FORCE>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+    if (rc.skip) return;
+    sfor<0, NV>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        constexpr double w = wgt<double>(i);
-        const double t = ((fator * w) * rho) * cosp[i];
-        fR[i] = conc_R * f[i] - t;
-        fB[i] = conc_B * f[i] + t;
+        split64<i>(rc, f[i], fR[i], fB[i]);
     });
 }
 
 // ---------------------------------------------------------------------------------------------
 // FP32 shifted form: e_i = f_i - w_i rho0, d_i = f_R,i - f_B,i
 // ---------------------------------------------------------------------------------------------
+// Recolouring split of the FP32 form: d_i = rho^N f_i - fat2 w_i cos(phi_i) with
+// fat2 = 2 beta c_R c_B rho = beta (1 - rho^N^2) rho / 2 (c_R - c_B = rho^N).
+struct Recolour32 {
+    float phi, fat2, gx, gy, gz, inv_mod;
+    bool skip;
+};
+
+template <int i>
+__device__ __forceinline__ float split32(const Recolour32 &r, float ei, float rho0) {
+    constexpr float w = wgt<float>(i);
+    const float f = w * rho0 + ei;
+    if constexpr (i == 0) {
+        return r.phi * f;
+    } else {
+        constexpr float rs2 = 0.70710678118654752f;
+        const float cg = (float)cx(i) * r.gx + (float)cy(i) * r.gy + (float)cz(i) * r.gz;
+        const float cosp = cg * r.inv_mod * (cc(i) == 2 ? rs2 : 1.0f);
+        return r.phi * f - r.fat2 * w * cosp;
+    }
+}
+
+// e_i = f_i - w_i rho0 in, post-collision e_i out; drho = sum e_i, D = sum d_i = rho_R - rho_B.
 template <bool FORCE>
-__device__ __forceinline__ void collide_f32(float (&e)[NV], float (&d)[NV], float drho, float D,
-                                            float gmx, float gmy, float gmz, float Fx, float Fy,
-                                            float Fz, const CaseDev &c) {
+__device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D, float gmx,
+                                            float gmy, float gmz, float Fx, float Fy, float Fz,
+                                            const CaseDev &c, Recolour32 &rc) {
     const float rho0 = (float)c.rho0;
     const float rho = rho0 + drho;
-    if (rho <= 1.0e-30f) return;
+    rc.skip = !(rho > 1.0e-30f);
+    if (rc.skip) return;
     const float inv_rho = 1.0f / rho;
     const float phi = D * inv_rho;  // rho^N = (rho_R - rho_B) / rho
     float ax = 0.f, ay = 0.f, az = 0.f;
@@ -238,22 +315,12 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float (&d)[NV], floa
             });
         }
     }
-    // recolour: d_i = (c_R - c_B) f_i - 2 beta c_R c_B w_i rho cos(phi_i), c_R - c_B = rho^N
-    const float fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
-    const float inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
-    constexpr float rs2 = 0.70710678118654752f;
-    sfor<0, NV>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        constexpr float w = wgt<float>(i);
-        const float f = w * rho0 + e[i];
-        if constexpr (i == 0) {
-            d[i] = phi * f;
-        } else {
-            const float cg = (float)cx(i) * gmx + (float)cy(i) * gmy + (float)cz(i) * gmz;
-            const float cosp = cg * inv_mod * (cc(i) == 2 ? rs2 : 1.0f);
-            d[i] = phi * f - fat2 * w * cosp;
-        }
-    });
+    rc.phi = phi;
+    rc.fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
+    rc.inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
+    rc.gx = gmx;
+    rc.gy = gmy;
+    rc.gz = gmz;
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -31,41 +31,13 @@ __device__ __forceinline__ int wrapi(int a, int n) {
 template <class S>
 struct SmemT {
     S phi[PY][PX];        // rho^N of tile + halo (HMAX), position (px, py) = global (x0-2+px, y0-2+py)
+    S rsum[2][PY * PX - TX * TY];  // halo ring: the two colour sums of each ring node
     S g[QY][QX][3];       // ring-1 gradient (F1, F2)
     S aux[QY][QX][6];     // ring-1 normal (F1) or stress (F2)
 };
 
-// ---- loads ------------------------------------------------------------------------------------
-// FP64: sums rho_R, rho_B in index order (density(), LBM_functions.cpp:1582-1590) and
-// rho^N = (rho_R - rho_B) / (rho_R + rho_B) as at Imm_OPS.cpp:255-258.
-__device__ __forceinline__ void load_node(const double *__restrict__ src, long long stride,
-                                          long long off, double (&a)[NV], double (&b)[NV],
-                                          double &sa, double &sb) {
-    sa = 0.0;
-    sb = 0.0;
-#pragma unroll
-    for (int i = 0; i < NV; i++) a[i] = __ldg(src + (long long)i * stride + off);
-#pragma unroll
-    for (int i = 0; i < NV; i++) b[i] = __ldg(src + (long long)(NV + i) * stride + off);
-#pragma unroll
-    for (int i = 0; i < NV; i++) sa = sa + a[i];
-#pragma unroll
-    for (int i = 0; i < NV; i++) sb = sb + b[i];
-}
-__device__ __forceinline__ void load_node(const float *__restrict__ src, long long stride,
-                                          long long off, float (&a)[NV], float (&b)[NV], float &sa,
-                                          float &sb) {
-    sa = 0.f;
-    sb = 0.f;
-#pragma unroll
-    for (int i = 0; i < NV; i++) a[i] = __ldg(src + (long long)i * stride + off);
-#pragma unroll
-    for (int i = 0; i < NV; i++) b[i] = __ldg(src + (long long)(NV + i) * stride + off);
-#pragma unroll
-    for (int i = 0; i < NV; i++) sa += a[i];
-#pragma unroll
-    for (int i = 0; i < NV; i++) sb += b[i];
-}
+// rho^N from the two colour sums.  FP64: (rho_R - rho_B) / (rho_R + rho_B), Imm_OPS.cpp:255-258.
+// FP32: the sums are sum e_i (rho - rho0) and sum d_i (rho_R - rho_B).
 __device__ __forceinline__ double phase_of(double rR, double rB, const CaseDev &) {
     return (rR - rB) / (rR + rB);
 }
@@ -73,19 +45,8 @@ __device__ __forceinline__ float phase_of(float drho, float D, const CaseDev &c)
     return D / ((float)c.rho0 + drho);
 }
 
-// rho^N of one node, without keeping its populations (halo nodes).
-template <class S>
-__device__ __forceinline__ S phase_at(const S *__restrict__ src, long long stride, long long off,
-                                      const CaseDev &c) {
-    S sa = S(0), sb = S(0);
-#pragma unroll
-    for (int i = 0; i < NV; i++) sa = sa + __ldg(src + (long long)i * stride + off);
-#pragma unroll
-    for (int i = 0; i < NV; i++) sb = sb + __ldg(src + (long long)(NV + i) * stride + off);
-    return phase_of(sa, sb, c);
-}
-
-// ring position r -> staged-tile coordinates (px, py) for a halo of H around the TX x TY interior
+// ring position r -> staged-tile coordinates (px, py) for a halo of H around the TX x TY interior;
+// consecutive r run along x in the top and bottom bands, so loads of consecutive r coalesce
 __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
     const int W = TX + 2 * H;
     const int nTop = H * W;
@@ -104,16 +65,14 @@ __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
     }
 }
 
-template <class S, bool FORCE>
-__device__ __forceinline__ void collide(S (&a)[NV], S (&b)[NV], S sa, S sb, S gx, S gy, S gz,
-                                        S Fx, S Fy, S Fz, const CaseDev &c) {
-    if constexpr (std::is_same<S, double>::value)
-        collide_f64<FORCE>(a, b, sa, sb, gx, gy, gz, Fx, Fy, Fz, c);
-    else
-        collide_f32<FORCE>(a, b, sa, sb, gx, gy, gz, Fx, Fy, Fz, c);
-}
-
 // One tile of one case.
+//   phase A  each thread loads its node: FP64 keeps f_i = f_R,i + f_B,i and the colour sums (all
+//            colisao_comum needs, Operadores_tensao.cpp:343-360), FP32 keeps e_i and the sums;
+//            the halo ring is loaded as (ring node, colour) items spread over all threads, each an
+//            ordered sum of 19 values;
+//   phase A2 rho^N of the ring from the sums;
+//   phase B  F1 / F2: gradient and normal or stress on the ring-1 region;
+//   phase C  mediator gradient, force, collision, recolouring, push to x + c_i.
 template <class S>
 __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int aux_k,
                                           SmemT<S> &sm) {
@@ -129,24 +88,55 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     S *__restrict__ dst = (S *)c.buf[cur ^ 1];
     const int tipo = c.tipo;
 
-    // ---- phase A: own node (kept in registers) and rho^N of tile + halo -----------------------
+    // ---- phase A ----------------------------------------------------------------------------
     const int x = x0 + lx, y = y0 + ly;
     const bool valid = (x < xe) && (y < ye);
-    S a[NV], b[NV], sa = S(0), sb = S(0);
+    S f[NV], sa = S(0), sb = S(0);
     if (x < xe + H && y < ye + H) {
         const int xw = valid ? x : wrapi(x, nx), yw = valid ? y : wrapi(y, ny);
-        load_node(src, stride, (long long)yw * pitch + xw, a, b, sa, sb);
+        const long long off = (long long)yw * pitch + xw;
+        S a[NV], b[NV];
+#pragma unroll
+        for (int i = 0; i < NV; i++) a[i] = __ldg(src + (long long)i * stride + off);
+#pragma unroll
+        for (int i = 0; i < NV; i++) b[i] = __ldg(src + (long long)(NV + i) * stride + off);
+#pragma unroll
+        for (int i = 0; i < NV; i++) sa = sa + a[i];
+#pragma unroll
+        for (int i = 0; i < NV; i++) sb = sb + b[i];
+        if constexpr (std::is_same<S, double>::value) {
+#pragma unroll
+            for (int i = 0; i < NV; i++) f[i] = a[i] + b[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < NV; i++) f[i] = a[i];
+        }
         sm.phi[ly + HMAX][lx + HMAX] = phase_of(sa, sb, c);
     }
     const int nring = (TX + 2 * H) * (TY + 2 * H) - TX * TY;
-    for (int r = tid; r < nring; r += STEP_THREADS) {
+    for (int it = tid; it < 2 * nring; it += STEP_THREADS) {
+        const int colour = it / nring, r = it - colour * nring;
         int px, py;
         ring_pos(r, H, px, py);
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
         if (gx < xe + H && gy < ye + H) {
-            const int xw = wrapi(gx, nx), yw = wrapi(gy, ny);
-            sm.phi[py][px] = phase_at(src, stride, (long long)yw * pitch + xw, c);
+            const long long off = (long long)wrapi(gy, ny) * pitch + wrapi(gx, nx);
+            const S *p = src + (long long)(colour * NV) * stride + off;
+            S v[NV];
+#pragma unroll
+            for (int i = 0; i < NV; i++) v[i] = __ldg(p + (long long)i * stride);
+            S acc = S(0);
+#pragma unroll
+            for (int i = 0; i < NV; i++) acc = acc + v[i];
+            sm.rsum[colour][r] = acc;
         }
+    }
+    __syncthreads();
+    for (int r = tid; r < nring; r += STEP_THREADS) {
+        int px, py;
+        ring_pos(r, H, px, py);
+        const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
+        if (gx < xe + H && gy < ye + H) sm.phi[py][px] = phase_of(sm.rsum[0][r], sm.rsum[1][r], c);
     }
     __syncthreads();
 
@@ -193,20 +183,53 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             Fy = mu * g1;
             Fz = mu * g2;
         }
-        if (force) collide<S, true>(a, b, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c);
-        else collide<S, false>(a, b, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c);
-
-        // push to x + c_i (periodic)
         const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
         const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
-        sfor<0, NV>([&](auto I) {
-            constexpr int i = decltype(I)::value;
+        auto dst_off = [&](int i) {
             const int xd = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
             const int yd = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
-            const long long o = (long long)yd * pitch + xd;
-            dst[(long long)i * stride + o] = a[i];
-            dst[(long long)(NV + i) * stride + o] = b[i];
-        });
+            return (long long)yd * pitch + xd;
+        };
+        bool skip;
+        if constexpr (std::is_same<S, double>::value) {
+            Recolour64 rc;
+            if (force) collide_f64<true>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+            else collide_f64<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+            skip = rc.skip;
+            if (!skip) {
+                sfor<0, NV>([&](auto I) {
+                    constexpr int i = decltype(I)::value;
+                    double r, b;
+                    split64<i>(rc, f[i], r, b);
+                    const long long o = dst_off(i);
+                    dst[(long long)i * stride + o] = r;
+                    dst[(long long)(NV + i) * stride + o] = b;
+                });
+            }
+        } else {
+            Recolour32 rc;
+            if (force) collide_f32<true>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+            else collide_f32<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+            skip = rc.skip;
+            if (!skip) {
+                const float rho0 = (float)c.rho0;
+                sfor<0, NV>([&](auto I) {
+                    constexpr int i = decltype(I)::value;
+                    const long long o = dst_off(i);
+                    dst[(long long)i * stride + o] = f[i];
+                    dst[(long long)(NV + i) * stride + o] = split32<i>(rc, f[i], rho0);
+                });
+            }
+        }
+        if (skip) {  // rho <= 1e-30: the site is streamed unchanged (Operadores_tensao.cpp:347)
+            const long long off = (long long)y * pitch + x;
+            sfor<0, NV>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                const long long o = dst_off(i);
+                dst[(long long)i * stride + o] = src[(long long)i * stride + off];
+                dst[(long long)(NV + i) * stride + o] = src[(long long)(NV + i) * stride + off];
+            });
+        }
 
         if (c.aux != nullptr && (k == aux_k || (c.aux_at_end && k == c.chunk_len - 1))) {
             const long long o = (long long)y * pitch + x;
@@ -220,8 +243,16 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     __syncthreads();
 }
 
+// Resident CTAs per SM the register allocation is sized for: 2 x 256 threads for FP64, 4 x 256
+// threads for FP32 (the kernel is latency-bound at lower occupancy; see the ncu summaries).
+#ifdef ITLBM_STEP_F64
+#define ITLBM_STEP_MIN_BLOCKS 2
+#else
+#define ITLBM_STEP_MIN_BLOCKS 4
+#endif
+
 template <class S>
-__global__ void __launch_bounds__(STEP_THREADS) k_step(const CaseDev *__restrict__ cases,
+__global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(const CaseDev *__restrict__ cases,
                                                        const TileRef *__restrict__ tiles,
                                                        int ntiles, const int *__restrict__ ntiles_dev,
                                                        int k, int aux_k) {
@@ -246,12 +277,22 @@ cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int 
     k_step<double><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
     return cudaGetLastError();
 }
+int step_occupancy_f64() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<double>, STEP_THREADS, 0);
+    return n;
+}
 #else
 cudaError_t launch_step_f32(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s) {
     if (grid <= 0) return cudaSuccess;
     k_step<float><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
     return cudaGetLastError();
+}
+int step_occupancy_f32() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<float>, STEP_THREADS, 0);
+    return n;
 }
 #endif
 

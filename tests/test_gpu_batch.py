@@ -1,0 +1,105 @@
+"""The batched engine: every case gives the same bits alone and in a mixed batch (cases of
+different sizes, operators, precisions and geometries, admitted at different times), its
+diagnostics fall on the reference's steps (every 500 steps and the last), and the admission
+budget is honoured."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def mkdesc(itlbm, nx, tipo, chi=0.5, xi=1.569988, A=0.1, tau=0.8, prec=0, geometry=0, p=1, q=0, v0=0.0):
+    op = itlbm.make_op(tipo, chi, xi)
+    return itlbm.desc(nx, nx, op, tau=tau, A_fact=A, precision=prec, geometry=geometry, p=p, q=q, v0=v0)
+
+
+MIX = [  # (nx, tipo, chi, A, prec, geometry, pq, steps)
+    (48, 3, 0.5, 0.225, 0, 0, (1, 0), 1001),
+    (37, 12, 0.5, 0.1, 1, 0, (1, 0), 777),
+    (64, 11, 0.5, 0.1, 1, 1, (2, 1), 600),
+    (33, 13, 0.5, 0.1, 0, 0, (1, 0), 1200),
+    (80, 1, 0.5, 0.225, 1, 0, (1, 0), 501),
+    (40, 3, 2.0, 0.225, 0, 1, (1, 1), 1),
+]
+
+
+def run_alone(itlbm, d, steps):
+    """Same schedule as the batch: diagnostics at multiples of 500 and at the last step."""
+    rows = []
+    with itlbm.Case(d) as c:
+        s = 0
+        while s < steps:
+            nxt = min(((s + 499) // 500) * 500, steps - 1)
+            c.step(nxt - s + 1, keep_aux=True)
+            rows.append(c.diag_drop(nxt).as_dict() if d.geometry == 0 else c.diag_strip(nxt).as_dict())
+            s = nxt + 1
+        return rows, c.read_pops(0)
+
+
+def test_batch_equals_alone(gpu):
+    descs = [mkdesc(gpu, nx, t, chi, A=A, prec=pr, geometry=g, p=pq[0], q=pq[1]) for nx, t, chi, A, pr, g, pq, _ in MIX]
+    alone = [run_alone(gpu, d, m[-1]) for d, m in zip(descs, MIX)]
+    with gpu.Batch(chunk=200) as b:
+        # half submitted now, half after the first round
+        for k in range(0, len(MIX), 2):
+            b.submit(descs[k], MIX[k][-1], k)
+        b.advance()
+        for k in range(1, len(MIX), 2):
+            b.submit(descs[k], MIX[k][-1], k)
+        events = []
+        for _ in range(200):
+            b.advance()
+            events += b.poll()
+            st = b.stats()
+            if st.active == 0 and st.pending == 0:
+                break
+        assert st.finished == len(MIX)
+    for k, (rows, _) in enumerate(alone):
+        diag = [e for e in events if e.tag == k and e.kind == gpu.EV_DIAG]
+        done = [e for e in events if e.tag == k and e.kind == gpu.EV_DONE]
+        assert len(done) == 1 and done[0].step == MIX[k][-1]
+        assert [e.step for e in diag] == [r["step"] for r in rows]
+        for e, r in zip(diag, rows):
+            got = (e.drop if MIX[k][5] == 0 else e.strip).as_dict()
+            assert got == r, (k, {f: (got[f], r[f]) for f in r if got[f] != r[f]})
+
+
+def test_admission_budget(gpu):
+    d = mkdesc(gpu, 256, 3, A=0.225, prec=1)
+    per_case = 2 * 2 * 19 * 256 * 256 * 4
+    with gpu.Batch(hbm_budget=int(2.5 * per_case), chunk=100) as b:
+        for k in range(5):
+            b.submit(d, 150, k)
+        b.advance()
+        st = b.stats()
+        assert st.active == 2 and st.pending == 3 and st.hbm_used <= 2.5 * per_case
+        for _ in range(50):
+            b.advance()
+            st = b.stats()
+            if st.finished == 5:
+                break
+        assert st.finished == 5 and st.hbm_used == 0
+        with pytest.raises(gpu.ItlbmError) as e:
+            b.submit(mkdesc(gpu, 1024, 3, prec=1), 10, 99)
+        assert e.value.code == -6
+
+
+def test_unstable_case_retires(gpu):
+    """P3 chi = -0.4, tau = 0.51, sigma = 1 blows up at step 500 (stored batch E4): reported unstable
+    there, the other case carries on."""
+    bad = mkdesc(gpu, 100, 3, chi=-0.4, A=9 * 1.0 / (4 * 0.51), tau=0.51, prec=0)
+    good = mkdesc(gpu, 48, 3, A=0.225, tau=1.0, prec=0)
+    with gpu.Batch(chunk=500) as b:
+        b.submit(bad, 20000, 1)
+        b.submit(good, 1500, 2)
+        ev = []
+        for _ in range(100):
+            b.advance()
+            ev += b.poll()
+            if b.stats().finished == 2:
+                break
+    kinds = {(e.tag, e.kind) for e in ev}
+    assert (1, gpu.EV_UNSTABLE) in kinds and (2, gpu.EV_DONE) in kinds
+    assert [e.step for e in ev if e.tag == 1 and e.kind == gpu.EV_UNSTABLE] == [500]

@@ -3,17 +3,23 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-Default workload: one 4096 x 4096 x 1 periodic box, static drop R = 400, operator P3 chi = 0.5,
-A = 0.225, tau = 1, beta = 0.8 (the single-case roofline configuration of the north star), stepped
-in FP32 shifted storage; the plain FP64 path (bit-identical to the reference) is measured on the
-same case beside it.  A "step" is one lattice-Boltzmann time step of the whole box.
+Default workload ("batch600"): the batched configuration of the north star -- 600 cases drawn from
+seed 20261203: square boxes with side log-uniform in 64-512, 80 % static drops (R uniform in 10 to
+side/4) and 20 % straight interfaces inclined at atan(q/p), p, q in 1..4; operator uniform over the
+seven; tau uniform in 0.51-2; sigma log-uniform in 0.1-2 (A = 9 sigma / 4 tau for class P); FP32
+shifted storage -- all advanced together by the batch engine (one CUDA graph of persistent step
+launches over the device work table).  A "step" is one lattice-Boltzmann time step of every case.
+Beside it, one 4096 x 4096 x 1 static drop (R = 400, P3 chi = 0.5, A = 0.225, tau = 1), the
+single-case roofline configuration, in FP32 and in the plain FP64 path (bit-identical to the
+reference).
 
-value   MLUPS (million lattice-node updates per second), device time from CUDA events on the
-        launching stream around exactly K steps, inputs resident in HBM.  The state (5.1 GB FP32,
-        10.2 GB FP64) is far larger than L2, so no flush is needed between steps.
-e2e     the same metric through the C ABI as a user runs a case: itlbm_case_create (the initial
-        profile is computed on the host and copied up), K steps with a diagnostic every 500 steps and
-        at the end (each one a device-to-host copy of the observables), wall clock.
+value   MLUPS (million lattice-node updates per second) of the batch, device time from CUDA events
+        on the batch's stream around exactly K steps, state resident in HBM (11+ GB, far larger than
+        L2, so no flush is needed between steps).
+e2e     the same metric through the C ABI as a user runs the batch: itlbm_batch_submit of every case
+        (the initial profiles are computed on the host and copied up), advances of up to 500 steps
+        with the diagnostics that fall due (each a device-to-host copy of the observables), wall
+        clock from the first submit to the last step.
 roofline algorithmic bytes per update: 38 populations read + 38 written (304 B in FP32, 608 B in
         FP64) x nodes / mean kernel duration, against the measured copy bandwidth.
 cpu_baseline the reference's own step (Imm_OPS.cpp:252-287, compiled from its sources with its own
@@ -44,6 +50,96 @@ def hbm_peak():
         return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
     except Exception:
         return HBM_FALLBACK, "fallback"
+
+
+def batch_mix(seed=20261203, n=600):
+    """The case mix of the batched configuration (see the module docstring)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ops = [(1, 0.5), (3, -0.4), (3, 0.5), (3, 2.0), (11, 0.5), (12, 0.5), (13, 0.5)]
+    cases = []
+    for _ in range(n):
+        side = int(round(math.exp(rng.uniform(math.log(64), math.log(512)))))
+        strip = rng.uniform() < 0.2
+        tipo, chi = ops[rng.integers(len(ops))]
+        tau = float(rng.uniform(0.51, 2.0))
+        sigma = float(math.exp(rng.uniform(math.log(0.1), math.log(2.0))))
+        A = 9.0 * sigma / (4.0 * tau) if tipo < 11 else sigma
+        p, q = (int(rng.integers(1, 5)), int(rng.integers(1, 5))) if strip else (1, 0)
+        radius = float(rng.uniform(10.0, side / 4.0)) if not strip else 0.0
+        steps = int(rng.integers(5000, 30001))
+        cases.append(dict(nx=side, tipo=tipo, chi=chi, tau=tau, A=A, strip=strip, p=p, q=q, radius=radius,
+                          steps=steps))
+    return cases
+
+
+def batch_desc(pkg, c, prec):
+    op = pkg.make_op(c["tipo"], c["chi"], 1.569988)
+    return pkg.desc(c["nx"], c["nx"], op, tau=c["tau"], beta=0.8, A_fact=c["A"], radius=c["radius"],
+                    geometry=pkg.GEOM_STRIP if c["strip"] else pkg.GEOM_DROP, p=c["p"], q=c["q"],
+                    precision=prec)
+
+
+def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600):
+    """MLUPS of the batch over exactly `steps` steps of every case (one graph replay)."""
+    import torch
+    mix = batch_mix(n=n_cases)
+    nodes = sum(c["nx"] * c["nx"] for c in mix)
+    b = pkg.Batch(chunk=steps, diag_every=10 ** 9)
+    for k, c in enumerate(mix):
+        b.submit(batch_desc(pkg, c, pkg.PREC_F32), 10 ** 8, k)
+    b.advance()  # admission, step 0 and its diagnostic
+    st = b.stats()
+    assert st.active == n_cases, f"only {st.active} of {n_cases} cases admitted"
+    b.advance()  # warm-up replay
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    st0 = b.stats()
+    sampler = ClockSampler(local) if sample_clocks else None
+    if sampler:
+        sampler.__enter__()
+        time.sleep(0.3)
+    b.advance()  # the timed replay: exactly `steps` steps of every case
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__()
+    barrier(world)
+    torch.cuda.synchronize()
+    st1 = b.stats()
+    ms = st1.device_ms - st0.device_ms
+    upd = st1.node_updates - st0.node_updates
+    assert upd == nodes * steps
+    b.close()
+    return nodes, ms, allreduce_max(ms, world), (sampler.summary() if sampler else None), len(mix)
+
+
+def batch_e2e(pkg, steps, n_cases=600):
+    """The batch through the C ABI, wall clock: submit every case, advance until each has run
+    `steps` steps (diagnostics every 500 steps fall due on the way), poll the events."""
+    import ctypes
+    mix = batch_mix(n=n_cases)
+    nodes = sum(c["nx"] * c["nx"] for c in mix)
+    t0 = time.perf_counter()
+    b = pkg.Batch(chunk=500, diag_every=500)
+    for k, c in enumerate(mix):
+        b.submit(batch_desc(pkg, c, pkg.PREC_F32), steps, k)
+    nev = 0
+    while True:
+        b.advance()
+        nev += len(b.poll())
+        st = b.stats()
+        if st.active == 0 and st.pending == 0:
+            break
+    dt = time.perf_counter() - t0
+    upd = st.node_updates
+    b.close()
+    h2d = 8 * nodes
+    d2h = nev * ctypes.sizeof(pkg.BatchEvent)
+    return {"value": upd / dt / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "wall_s": dt, "events": nev,
+            "note": "whole batch through itlbm_batch_*: host profiles up, diagnostics down; unstable "
+                    "cases retire early, so node updates are counted, not assumed"}
 
 
 WORKLOADS = {
@@ -238,7 +334,7 @@ def main():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="drop4096", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="batch600", choices=["batch600"] + sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -255,21 +351,40 @@ def main():
     w = WORKLOADS[args.workload]
     peak, peak_kind = hbm_peak()
 
-    # headline: FP32 shifted storage
-    n, ms, ms_max, clocks = device_run(pkg, w, pkg.PREC_F32, args.steps, args.warmup, world, rank == 0, local)
-    mlups = allreduce_sum(n * args.steps, world) / (ms_max * 1e-3) / 1e6
-    bytes_lu = 304.0
-    achieved = bytes_lu * n * args.steps / (ms * 1e-3) / 1e9
-    # plain FP64 on the same case
-    n64, ms64, ms64_max, _ = device_run(pkg, w, pkg.PREC_F64, max(50, args.steps // 4), args.warmup,
-                                        world, False, local)
-    k64 = max(50, args.steps // 4)
-    mlups64 = allreduce_sum(n64 * k64, world) / (ms64_max * 1e-3) / 1e6
-    achieved64 = 608.0 * n64 * k64 / (ms64 * 1e-3) / 1e9
+    single = WORKLOADS["drop4096" if args.workload == "batch600" else args.workload]
+    if args.workload == "batch600":
+        nodes, ms, ms_max, clocks, ncases = batch_run(pkg, args.steps, args.warmup, world, rank == 0, local)
+        mlups = allreduce_sum(nodes * args.steps, world) / (ms_max * 1e-3) / 1e6
+        achieved = 304.0 * nodes * args.steps / (ms * 1e-3) / 1e9
+        launches = 2 * args.steps  # one FP64 and one FP32 persistent launch per step (no FP64 cases here)
+        cfg = {"workload": "batch600: 600 cases (seed 20261203), side 64-512 log-uniform, 80% drops / 20% "
+                           "inclined strips, 7 operators, tau 0.51-2, sigma 0.1-2, FP32 shifted storage",
+               "nodes": nodes, "cases": ncases,
+               "l2": "state 11+ GB >> 126 MB L2: no flush needed", "parallelism": f"replicas x{world}"}
+    else:
+        nodes, ms, ms_max, clocks = device_run(pkg, single, pkg.PREC_F32, args.steps, args.warmup, world,
+                                               rank == 0, local)
+        mlups = allreduce_sum(nodes * args.steps, world) / (ms_max * 1e-3) / 1e6
+        achieved = 304.0 * nodes * args.steps / (ms * 1e-3) / 1e9
+        launches = args.steps
+        cfg = {"workload": f"{args.workload}: {single['nx']}x{single['ny']}x1 static drop, P3 chi=0.5, FP32",
+               "nodes": nodes, "parallelism": f"replicas x{world}"}
 
-    e2e = None if args.no_e2e else e2e_run(pkg, w, pkg.PREC_F32, args.steps)
-    if e2e and world > 1:
-        e2e["value"] = allreduce_sum(e2e["value"], world)
+    # the single 4096^2 case, FP32 and plain FP64
+    ks = max(50, args.steps // 2)
+    n1, ms1, ms1_max, _ = device_run(pkg, single, pkg.PREC_F32, ks, args.warmup, world, False, local)
+    n64, ms64, ms64_max, _ = device_run(pkg, single, pkg.PREC_F64, ks, args.warmup, world, False, local)
+    single32 = {"value": allreduce_sum(n1 * ks, world) / (ms1_max * 1e-3) / 1e6, "unit": "MLUPS", "steps": ks,
+                "roofline_frac": 304.0 * n1 * ks / (ms1 * 1e-3) / 1e9 / peak}
+    fp64 = {"value": allreduce_sum(n64 * ks, world) / (ms64_max * 1e-3) / 1e6, "unit": "MLUPS", "steps": ks,
+            "roofline_frac": 608.0 * n64 * ks / (ms64 * 1e-3) / 1e9 / peak,
+            "workload": "4096x4096x1 static drop R=400, P3 chi=0.5, FP64 plain (bit-identical to the reference)"}
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = batch_e2e(pkg, 1001) if args.workload == "batch600" else e2e_run(pkg, single, pkg.PREC_F32, args.steps)
+        if world > 1:
+            e2e["value"] = allreduce_sum(e2e["value"], world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -279,17 +394,14 @@ def main():
             "metric": "MLUPS & % HBM roofline, batched FP32 vs plain FP64 on 1 B200; p99 case latency",
             "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {w['nx']}x{w['ny']}x1 static drop R={w['radius']:g}, "
-                                   f"P3 chi=0.5, A=0.225, tau=1, beta=0.8, FP32 shifted storage",
-                       "nodes": n, "l2": "state 5.1 GB/step (FP32) >> 126 MB L2: no flush needed",
-                       "parallelism": f"replicas x{world}"},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "bytes_per_lu": bytes_lu},
-            "fp64_plain": {"value": mlups64, "unit": "MLUPS", "steps": k64,
-                           "roofline": {"achieved": achieved64, "frac": achieved64 / peak, "bytes_per_lu": 608.0}},
-            "gpu_launches": args.steps,
+                         "bytes_per_lu": 304.0},
+            "fp32_single_4096": single32,
+            "fp64_plain": fp64,
+            "batched_fp32_over_plain_fp64": mlups / fp64["value"],
+            "gpu_launches": launches,
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,

@@ -232,9 +232,10 @@ __device__ __forceinline__ void colisao_site_f64(double (&fR)[NV], double (&fB)[
 // FP32 shifted form: e_i = f_i - w_i rho0, d_i = f_R,i - f_B,i
 // ---------------------------------------------------------------------------------------------
 // Recolouring split of the FP32 form: d_i = rho^N f_i - fat2 w_i cos(phi_i) with
-// fat2 = 2 beta c_R c_B rho = beta (1 - rho^N^2) rho / 2 (c_R - c_B = rho^N).
+// fat2 = 2 beta c_R c_B rho = beta (1 - rho^N^2) rho / 2 (c_R - c_B = rho^N); d_0 is the complement
+// D - sum_{i>=1} d_i (see collide_f32).
 struct Recolour32 {
-    float phi, fat2, gx, gy, gz, inv_mod;
+    float D, phi, fat2, gx, gy, gz, inv_mod;
     bool skip;
 };
 
@@ -315,6 +316,15 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
             });
         }
     }
+    // Every site update conserves the mass (sum e_i = drho) and the colour difference (sum d_i = D)
+    // exactly; in float arithmetic the weights do not sum to 1 (1 + 1.5e-8), which would bias both
+    // sums every step.  The rest populations e_0 and d_0 are therefore formed as the complements.
+    {
+        float s = 0.f;
+        sfor<1, NV>([&](auto I) { s += e[decltype(I)::value]; });
+        e[0] = drho - s;
+    }
+    rc.D = D;
     rc.phi = phi;
     rc.fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
     rc.inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;

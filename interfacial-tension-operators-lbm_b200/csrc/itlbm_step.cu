@@ -213,12 +213,18 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             skip = rc.skip;
             if (!skip) {
                 const float rho0 = (float)c.rho0;
-                sfor<0, NV>([&](auto I) {
+                float dsum = 0.f;
+                sfor<1, NV>([&](auto I) {
                     constexpr int i = decltype(I)::value;
                     const long long o = dst_off(i);
+                    const float d = split32<i>(rc, f[i], rho0);
+                    dsum += d;
                     dst[(long long)i * stride + o] = f[i];
-                    dst[(long long)(NV + i) * stride + o] = split32<i>(rc, f[i], rho0);
+                    dst[(long long)(NV + i) * stride + o] = d;
                 });
+                const long long o0 = dst_off(0);
+                dst[o0] = f[0];
+                dst[(long long)NV * stride + o0] = rc.D - dsum;
             }
         }
         if (skip) {  // rho <= 1e-30: the site is streamed unchanged (Operadores_tensao.cpp:347)

@@ -174,4 +174,31 @@ bool write_vtk_velocity(const std::string &path, int nx, int ny, const double *u
     return true;
 }
 
+double dist_central(int x, int y, int p, int q, int N) {
+    const double m = std::sqrt((double)(p * p + q * q));
+    long long s = ((long long)p * x + (long long)q * y) % N;
+    if (s < 0) s += N;
+    double d = ((double)s - 0.5 * N);
+    if (d >= 0.5 * N) d -= N;
+    if (d < -0.5 * N) d += N;
+    return -d / m;
+}
+
+bool write_perfil(const std::string &path, int N, int p, int q, const std::vector<double> &rR,
+                  const std::vector<double> &rB, const std::vector<double> &ux,
+                  const std::vector<double> &uy) {
+    std::ofstream fp(path);
+    if (!fp) return false;
+    fp << "# d  c=rho_R/rho  rho  ux  uy\n" << std::setprecision(10);
+    for (int y = 0; y < N; y++)
+        for (int x = 0; x < N; x++) {
+            const size_t k = (size_t)y * N + x;
+            const double rho = rR[k] + rB[k];
+            if (!(rho > 0)) continue;
+            const double dd = dist_central(x, y, p, q, N);
+            if (std::fabs(dd) < 12.0) fp << dd << " " << rR[k] / rho << " " << rho << " " << ux[k] << " " << uy[k] << "\n";
+        }
+    return true;
+}
+
 }  // namespace itlbm_host

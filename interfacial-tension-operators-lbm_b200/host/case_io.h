@@ -55,4 +55,13 @@ bool write_vtk_velocity(const std::string &path, int nx, int ny, const double *u
 
 std::string join(const std::string &dir, const std::string &file);
 
+// dist_central (Imm_INCL.cpp:74-83): signed distance to the central interface, > 0 on the red side
+double dist_central(int x, int y, int p, int q, int N);
+
+// perfil.dat (Imm_INCL.cpp:101, :162): d, c_R, rho, ux, uy of the nodes with |d| < 12, in y-major
+// order, from the post-collision fields of the last step
+bool write_perfil(const std::string &path, int N, int p, int q, const std::vector<double> &rR,
+                  const std::vector<double> &rB, const std::vector<double> &ux,
+                  const std::vector<double> &uy);
+
 }  // namespace itlbm_host

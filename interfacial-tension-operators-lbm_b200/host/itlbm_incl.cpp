@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "case_io.h"
+#include "case_run.h"
 
 #include <cuda_runtime.h>
 
@@ -24,19 +25,7 @@ using namespace itlbm_host;
 namespace {
 const double ESPESSURA_INI = 3.45;  // Imm_INCL.cpp:41
 const int PASSOS_DIAG = 500;        // Imm_INCL.cpp:42
-const double U_LIMITE = 0.4;        // Imm_INCL.cpp:43
 const double PI = 3.14159265358979323846;
-
-// dist_central (Imm_INCL.cpp:74-83): signed distance to the central interface
-double dist_central(int x, int y, int p, int q, int N) {
-    const double m = std::sqrt((double)(p * p + q * q));
-    long long s = ((long long)p * x + (long long)q * y) % N;
-    if (s < 0) s += N;
-    double d = ((double)s - 0.5 * N);
-    if (d >= 0.5 * N) d -= N;
-    if (d < -0.5 * N) d += N;
-    return -d / m;
-}
 
 int die(itlbm_case *c, int rc, const char *what) {
     std::cerr << "\n" << what << ": " << itlbm_last_error() << std::endl;
@@ -110,18 +99,8 @@ int main(int argc, char **argv) {
     itlbm_case *c = nullptr;
     if (itlbm_case_create(&d, &c) != ITLBM_OK) return die(c, 1, "itlbm_case_create");
 
-    std::ofstream f_inc(join(dir, "inclinada.dat"));
-    f_inc << std::setprecision(10);
-    f_inc << "# 1:passo  2:sigma_pop  3:int_grad  4:K  5:espessura_10_90  6:residuo  7:d0  8:|u|max  9:|u|rms"
-             "  10:|u_n|max  11:|u_t|max  12:massa_R  13:massa_B  14:qx  15:qy  16:soma_Fx  17:soma_Fy"
-             "  18:min_f  19:neg_total  20:neg_cor\n";
-
-    double s_sig = 0, s_um = 0, s_un = 0, s_ut = 0, s_K = 0, s_res = 0, s_ig = 0;
-    int n_med = 0;
-    long long neg_t = 0, neg_c = 0;
-    double min_f = 1e300, d0_ini = NAN, d0_fim = NAN;
-    std::string estado = "estavel";
-    int passo_falha = -1;
+    StripRun run;
+    if (!run.open(dir, din.n_steps, p, q)) return die(c, 1, "cannot write the output files");
     const int n_steps = din.n_steps;
     const auto t0 = std::chrono::steady_clock::now();
     int step = 0;
@@ -135,53 +114,14 @@ int main(int argc, char **argv) {
         if (step % PASSOS_DIAG == 0 || ultimo) {
             itlbm_strip_diag r;
             if (itlbm_case_diag_strip(c, step, &r, nullptr) != ITLBM_OK) return die(c, 2, "itlbm_case_diag_strip");
-            const bool ok = r.ok != 0;
             if (ultimo) {  // perfil.dat, Imm_INCL.cpp:101, :162
                 const size_t n = (size_t)N * N;
                 std::vector<double> rR(n), rB(n), ux(n), uy(n);
                 if (itlbm_case_read_fields(c, rR.data(), rB.data(), ux.data(), uy.data(), nullptr, nullptr) != ITLBM_OK)
                     return die(c, 2, "itlbm_case_read_fields");
-                std::ofstream fp(join(dir, "perfil.dat"));
-                fp << "# d  c=rho_R/rho  rho  ux  uy\n" << std::setprecision(10);
-                for (int y = 0; y < N; y++)
-                    for (int x = 0; x < N; x++) {
-                        const size_t k = (size_t)y * N + x;
-                        const double rho = rR[k] + rB[k];
-                        if (!(rho > 0)) continue;
-                        const double dd = dist_central(x, y, p, q, N);
-                        if (std::fabs(dd) < 12.0)
-                            fp << dd << " " << rR[k] / rho << " " << rho << " " << ux[k] << " " << uy[k] << "\n";
-                    }
+                write_perfil(join(dir, "perfil.dat"), N, p, q, rR, rB, ux, uy);
             }
-            f_inc << step << " " << r.sigma_pop << " " << r.int_grad << " " << r.K << " "
-                  << (r.K > 0 ? 2.0 * std::log(9.0) / r.K : 0.0) << " " << r.res << " " << r.d0 << " " << r.u_max
-                  << " " << r.u_rms << " " << r.un_max << " " << r.ut_max << " " << r.massa_R << " " << r.massa_B
-                  << " " << r.qx << " " << r.qy << " " << r.SFx << " " << r.SFy << " " << r.min_f << " "
-                  << r.neg_total << " " << r.neg_cor << "\n";
-            f_inc.flush();
-            if (step == 0) d0_ini = r.d0;
-            d0_fim = r.d0;
-            neg_t = std::max(neg_t, r.neg_total);
-            neg_c = std::max(neg_c, r.neg_cor);
-            min_f = std::min(min_f, r.min_f);
-            if (step >= n_steps / 2) {
-                s_sig += r.sigma_pop;
-                s_um += r.u_max;
-                s_un += r.un_max;
-                s_ut += r.ut_max;
-                s_K += r.K;
-                s_res += r.res;
-                s_ig += r.int_grad;
-                n_med++;
-            }
-            std::cout << "\rstep = " << step << "   sigma_pop = " << r.sigma_pop << "   K = " << r.K
-                      << "   |u|max = " << r.u_max << "   neg = " << r.neg_total << "        " << std::endl;
-            if (!ok || r.u_max > U_LIMITE) {
-                estado = "instavel";
-                passo_falha = step;
-                std::cout << "\nSimulacao instavel no passo " << step << std::endl;
-                break;
-            }
+            if (run.on_diag(step, r, &std::cout)) break;
         }
         step++;
     }
@@ -190,17 +130,11 @@ int main(int argc, char **argv) {
 
     const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     const double mlups = (elapsed > 0) ? (double)n_fluid * step / (elapsed * 1e6) : 0.0;
-    auto med = [&](double s) { return n_med ? s / n_med : NAN; };
-    std::ofstream f_res(join(dir, "resumo.dat"));
-    f_res << std::setprecision(10);
-    f_res << "# operador chi xi tau beta fat_R_B N p q theta sigma_nominal estado passo_falha passos "
-             "sigma_pop_med int_grad_med K_med residuo_med umax_med un_max_med ut_max_med umax/sigma_nominal "
-             "d0_ini d0_fim neg_total_max neg_cor_max min_f MLUPS\n";
-    f_res << op.nome << " " << op.chi << " " << op.xi << " " << tau << " " << din.recoll << " " << A_in << " " << N
-          << " " << p << " " << q << " " << theta << " " << sigma_nominal << " " << estado << " " << passo_falha << " "
-          << step << " " << med(s_sig) << " " << med(s_ig) << " " << med(s_K) << " " << med(s_res) << " "
-          << med(s_um) << " " << med(s_un) << " " << med(s_ut) << " " << med(s_um) / sigma_nominal << " " << d0_ini
-          << " " << d0_fim << " " << neg_t << " " << neg_c << " " << min_f << " " << mlups << "\n";
+    run.write_resumo(dir, op, tau, din.recoll, A_in, N, theta, sigma_nominal, step, mlups);
+    auto med = [&](double s) { return run.n_med ? s / run.n_med : NAN; };
+    const double s_sig = run.s_sig, s_ig = run.s_ig, s_K = run.s_K, s_um = run.s_um, s_un = run.s_un, s_ut = run.s_ut;
+    const double d0_ini = run.d0_ini, d0_fim = run.d0_fim;
+    const std::string &estado = run.estado;
     std::cout << "\n\n================ Resultado ================" << std::endl;
     std::cout << "   estado            = " << estado << std::endl;
     std::cout << "   theta             = " << theta << " graus" << std::endl;

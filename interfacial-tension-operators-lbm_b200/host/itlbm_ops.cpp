@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "case_io.h"
+#include "case_run.h"
 
 #include <cuda_runtime.h>
 
@@ -28,7 +29,6 @@ using namespace itlbm_host;
 
 namespace {
 const int PASSOS_DIAG = 500;      // Imm_OPS.cpp:44
-const double U_LIMITE = 0.4;      // Imm_OPS.cpp:45
 
 int die(itlbm_case *c, int rc, const char *what) {
     std::cerr << "\n" << what << ": " << itlbm_last_error() << std::endl;
@@ -108,26 +108,8 @@ int main(int argc, char **argv) {
     itlbm_case *c = nullptr;
     if (itlbm_case_create(&d, &c) != ITLBM_OK) return die(c, 1, "itlbm_case_create");
 
-    std::ofstream f_lap(join(dir, "laplace.dat"));
-    f_lap << std::setprecision(10);
-    f_lap << "# 1:passo  2:raio_area  3:raio_grad  4:raio_linha  5:p_in  6:p_out  7:delta_p"
-             "  8:sigma  9:|u-v0|max  10:|u-v0|rms  11:Ca  12:massa_R  13:massa_B  14:|q|"
-             "  15:sd_p_in  16:sd_p_out  17:sigma_2pontos"
-             "  18:K_perfil  19:r_perfil  20:espessura_10_90  21:residuo_ajuste  22:n_camadas\n";
-    std::ofstream f_iso(join(dir, "iso.dat"));
-    f_iso << std::setprecision(10);
-    f_iso << "# 1:passo  2:R0  3:|a2|/R0  4:|a4|/R0  5:|a8|/R0  6:rmin  7:rmax\n";
-    std::ofstream f_gi(join(dir, "galilean.dat"));
-    gi_header(f_gi);
-
-    const double cs2 = 1. / 3.;
-    const double nu = cs2 * (tau - 0.5);
-    double s_sigma = 0, s_umax = 0, s_urms = 0, s_a4 = 0, s_a8 = 0, s_K = 0;
-    int n_med = 0;
-    long long neg_total_max = 0, neg_cor_max = 0;
-    double min_f_global = 1e30;
-    std::string estado = "estavel";
-    int passo_falha = -1;
+    DropRun run;
+    if (!run.open(dir, tau, v0, din.n_steps)) return die(c, 1, "cannot write the output files");
     const int n_steps = din.n_steps, n_files = din.n_files;
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<double> rR, rB, ux, uy, uz;
@@ -149,43 +131,7 @@ int main(int argc, char **argv) {
             itlbm_drop_diag dg;
             if (itlbm_case_diag_drop(c, step, x0_ini, y0_ini, &dg, nullptr) != ITLBM_OK)
                 return die(c, 2, "itlbm_case_diag_drop");
-            const bool ok = dg.ok != 0;
-            if (ok) {
-                const double Ca = (dg.sigma > 0.0) ? nu * dg.u_max / dg.sigma : 0.0;
-                const double q = std::sqrt(dg.qx * dg.qx + dg.qy * dg.qy + dg.qz * dg.qz);
-                f_lap << step << " " << dg.raio << " " << dg.raio_grad << " " << dg.raio_linha << " " << dg.p_in
-                      << " " << dg.p_out << " " << dg.delta_p << " " << dg.sigma << " " << dg.u_max << " "
-                      << dg.u_rms << " " << Ca << " " << dg.massa_R << " " << dg.massa_B << " " << q << " "
-                      << dg.sd_in << " " << dg.sd_out << " " << dg.sigma_linha << " " << dg.K_perfil << " "
-                      << dg.r_perfil << " " << dg.esp_perfil << " " << dg.res_perfil << " " << dg.n_perfil << "\n";
-                f_lap.flush();
-                gi_write(f_gi, step, v0, cs2, dg);
-                f_iso << step << " " << dg.R0 << " " << dg.a2 << " " << dg.a4 << " " << dg.a8 << " " << dg.rmin
-                      << " " << dg.rmax << "\n";
-                f_iso.flush();
-                neg_total_max = std::max(neg_total_max, dg.negative_total);
-                neg_cor_max = std::max(neg_cor_max, dg.negative_color);
-                min_f_global = std::min(min_f_global, dg.min_f);
-                if (step >= n_steps / 2) {
-                    s_sigma += dg.sigma;
-                    s_umax += dg.u_max;
-                    s_urms += dg.u_rms;
-                    s_a4 += dg.a4;
-                    s_a8 += dg.a8;
-                    s_K += dg.K_perfil;
-                    n_med++;
-                }
-                std::cout << "\rstep = " << step << "   R = " << dg.raio << "   sigma = " << dg.sigma
-                          << "   |u|max = " << dg.u_max << "   a4 = " << dg.a4 << "   neg = " << dg.negative_total
-                          << "        " << std::endl;
-            }
-            // Imm_OPS.cpp:346-352
-            if (!ok || dg.n_ruim > 0 || dg.u_max > U_LIMITE) {
-                estado = "instavel";
-                passo_falha = step;
-                std::cout << "\nSimulacao instavel no passo " << step << std::endl;
-                break;
-            }
+            if (run.on_diag(step, dg, &std::cout)) break;
         }
         if (is_vtk(step)) {  // GRAVA_CAMPOS_FINAIS, Imm_OPS.cpp:357-364
             const size_t n = (size_t)nx * ny;
@@ -205,24 +151,14 @@ int main(int argc, char **argv) {
     // resumo.dat (Imm_OPS.cpp:376-394)
     const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     const double mlups = (elapsed > 0) ? (double)n_fluid * step / (elapsed * 1e6) : 0.0;
-    const double m_sigma = n_med ? s_sigma / n_med : NAN;
-    const double m_umax = n_med ? s_umax / n_med : NAN;
-    std::ofstream f_res(join(dir, "resumo.dat"));
-    f_res << std::setprecision(10);
-    f_res << "# operador chi xi tau beta fat_R_B v0 nx R_ini sigma_nominal estado passo_falha passos "
-             "sigma_med umax_med urms_med umax/sigma Ca_s=nu*umax/sigma a4_med a8_med K_med "
-             "neg_total_max neg_cor_max min_f MLUPS\n";
-    f_res << op.nome << " " << op.chi << " " << op.xi << " " << tau << " " << din.recoll << " " << A_in << " " << v0
-          << " " << nx << " " << raio_ini << " " << sigma_nominal << " " << estado << " " << passo_falha << " "
-          << step << " " << m_sigma << " " << m_umax << " " << (n_med ? s_urms / n_med : NAN) << " "
-          << m_umax / m_sigma << " " << nu * m_umax / m_sigma << " " << (n_med ? s_a4 / n_med : NAN) << " "
-          << (n_med ? s_a8 / n_med : NAN) << " " << (n_med ? s_K / n_med : NAN) << " " << neg_total_max << " "
-          << neg_cor_max << " " << min_f_global << " " << mlups << "\n";
+    run.write_resumo(dir, op, tau, din.recoll, A_in, nx, raio_ini, sigma_nominal, step, mlups);
+    const double m_sigma = run.n_med ? run.s_sigma / run.n_med : NAN;
+    const double m_umax = run.n_med ? run.s_umax / run.n_med : NAN;
     std::cout << "\n\n================ Resultado ================" << std::endl;
-    std::cout << "   estado            = " << estado << std::endl;
+    std::cout << "   estado            = " << run.estado << std::endl;
     std::cout << "   sigma ( media )   = " << m_sigma << "   ( nominal " << sigma_nominal << " )" << std::endl;
     std::cout << "   |u|max ( media )  = " << m_umax << "   |u|max / sigma = " << m_umax / m_sigma << std::endl;
-    std::cout << "   populacoes < 0    = " << neg_total_max << " ( total )  " << neg_cor_max << " ( cor )" << std::endl;
+    std::cout << "   populacoes < 0    = " << run.neg_total_max << " ( total )  " << run.neg_cor_max << " ( cor )" << std::endl;
     std::cout << "   MLUPS             = " << mlups << std::endl;
     return 0;
 }

@@ -1,0 +1,306 @@
+// itlbm_serve -- continuous batching of case folders on one GPU.
+//
+//   itlbm_serve <spool-dir> [--budget-gb G] [--chunk K] [--fp64] [--idle-exit S] [--max-cases M]
+//
+// The reference runs one process per case folder (rodar_lote.py:231-243).  This server keeps one
+// batch (itlbm_batch_*) on the device and admits case folders as they arrive:
+//   * a request is a file <spool>/<name>.req whose first line is the path of a case folder (the
+//     folder rodar_lote.monta writes: data_in.txt, operador.txt, velocity.txt, meio.vtk and, for the
+//     inclined interface, inclinacao.txt); an optional second word "fp64" or "fp32" picks the storage;
+//   * the server renames it <name>.run, validates the folder like Imm_OPS / Imm_INCL (an invalid folder
+//     gets <name>.err with the message, the reference's exit code 1), and submits the case;
+//   * requests that arrive while others run are admitted as memory and slots free up: every round is
+//     one graph replay of all admitted cases, so their work overlaps on the device;
+//   * diagnostic rows stream into the case folder as they fall due (laplace.dat, iso.dat, galilean.dat
+//     or inclinada.dat, formats of the reference); at its last step or when the stop rule fires the
+//     case retires, resumo.dat is written (rodar_lote.feito's completion test) and <name>.run becomes
+//     <name>.done with its time-to-result;
+//   * <spool>/serve_stats.json keeps the count, p50 / p99 time-to-result and the aggregate MLUPS.
+// The client bin/itlbm_submit turns this into a drop-in for the Imm_OPS binary of rodar_lote.py.
+// The final VTK fields and perfil.dat are written only by itlbm_ops / itlbm_incl.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <dirent.h>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <sys/stat.h>
+#include <thread>
+#include <unistd.h>
+#include <vector>
+
+#include "case_io.h"
+#include "case_run.h"
+
+using namespace itlbm_host;
+
+namespace {
+
+struct Job {
+    std::string name, dir;
+    itlbm_case_desc desc{};
+    bool strip = false;
+    int n_steps = 0, nx = 0;
+    double raio_ini = 0, sigma_nominal = 0, theta = 0, beta = 0, A = 0, tau = 0;
+    double t_submit = 0;
+    std::unique_ptr<DropRun> drop;
+    std::unique_ptr<StripRun> stp;
+};
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+std::vector<std::string> list_requests(const std::string &spool) {
+    std::vector<std::string> out;
+    DIR *d = opendir(spool.c_str());
+    if (!d) return out;
+    while (dirent *e = readdir(d)) {
+        const std::string n = e->d_name;
+        if (n.size() > 4 && n.compare(n.size() - 4, 4, ".req") == 0) out.push_back(n.substr(0, n.size() - 4));
+    }
+    closedir(d);
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+void write_text(const std::string &path, const std::string &text) {
+    std::ofstream f(path + ".tmp");
+    f << text;
+    f.close();
+    std::rename((path + ".tmp").c_str(), path.c_str());
+}
+
+// Reads and validates a case folder like Imm_OPS.cpp:65-135 / Imm_INCL.cpp:192-266.
+bool prepare(Job &j, bool fp64, std::string &err) {
+    std::ostringstream log;
+    DataIn din;
+    if (!read_data(j.dir, din, log)) {
+        err = "data_in.txt ausente";
+        return false;
+    }
+    itlbm_operador op;
+    if (itlbm_operador_read(join(j.dir, "operador.txt").c_str(), &op) != ITLBM_OK) {
+        err = "operador.txt ausente ou invalido.  Uma linha: P1 | P3 chi | F1 | F2 | F3 xi";
+        return false;
+    }
+    int p = 1, q = 0;
+    struct stat st;
+    j.strip = stat(join(j.dir, "inclinacao.txt").c_str(), &st) == 0;
+    double v0 = 0.0;
+    if (j.strip) {
+        if (!read_inclinacao(j.dir, p, q)) {
+            err = "inclinacao.txt: \"p q\" inteiros, nao ambos nulos.";
+            return false;
+        }
+    } else if (!read_velocity(j.dir, v0)) {
+        err = "velocity.txt invalido.";
+        return false;
+    }
+    if (std::fabs(din.tau_R - din.tau_B) > 1e-14) {
+        err = "tau_R e tau_B tem de ser iguais.";
+        return false;
+    }
+    int nx, ny, nz;
+    long long n_fluid;
+    if (!read_geometry(join(j.dir, din.geo_file), nx, ny, nz, n_fluid)) {
+        err = "Nao foi possivel abrir " + din.geo_file;
+        return false;
+    }
+    if (nz != 1 || n_fluid != (long long)nx * ny || (j.strip && nx != ny)) {
+        err = j.strip ? "Este programa requer caixa quadrada N x N x 1, toda fluida."
+                      : "Este programa requer caixa 2D periodica toda fluida ( nz = 1 ).";
+        return false;
+    }
+    double R_gota, espessura;
+    read_gota(j.dir, R_gota, espessura);
+    itlbm_case_desc &d = j.desc;
+    d.nx = nx;
+    d.ny = ny;
+    d.op = op;
+    d.tau = din.tau_R;
+    d.beta = din.recoll;
+    d.A_fact = din.A_fact;
+    d.rho_R = j.strip ? 1.0 : din.rho_ini_R;
+    d.rho_B = j.strip ? 1.0 : din.rho_ini_B;
+    d.geometry = j.strip ? ITLBM_GEOM_STRIP : ITLBM_GEOM_DROP;
+    j.raio_ini = (R_gota > 0.0) ? R_gota : 0.25 * (double)nx;
+    d.radius = j.raio_ini;
+    d.k_profile = (espessura > 0.0) ? 2.0 * std::log(9.0) / espessura : 0.0;
+    d.v0 = v0;
+    d.p = p;
+    d.q = q;
+    d.precision = fp64 ? ITLBM_PREC_F64 : ITLBM_PREC_F32;
+    j.n_steps = din.n_steps;
+    j.nx = nx;
+    j.tau = din.tau_R;
+    j.beta = din.recoll;
+    j.A = din.A_fact;
+    j.sigma_nominal = op.tipo >= ITLBM_OP_F1 ? j.A : 4.0 / 9.0 * j.A * j.tau;
+    j.theta = std::atan2((double)q, (double)p) * 180.0 / 3.14159265358979323846;
+    if (j.n_steps < 1) {
+        err = "steps < 1";
+        return false;
+    }
+    if (j.strip) {
+        j.stp.reset(new StripRun());
+        if (!j.stp->open(j.dir, j.n_steps, p, q)) {
+            err = "cannot write inclinada.dat";
+            return false;
+        }
+    } else {
+        j.drop.reset(new DropRun());
+        if (!j.drop->open(j.dir, j.tau, v0, j.n_steps)) {
+            err = "cannot write the output files";
+            return false;
+        }
+    }
+    return true;
+}
+
+double percentile(std::vector<double> v, double p) {
+    if (v.empty()) return NAN;
+    std::sort(v.begin(), v.end());
+    const double r = p * (v.size() - 1);
+    const size_t i = (size_t)r;
+    const double f = r - i;
+    return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    if (argc < 2) {
+        std::cerr << "usage: itlbm_serve <spool-dir> [--budget-gb G] [--chunk K] [--fp64] [--idle-exit S] "
+                     "[--max-cases M]\n";
+        return 1;
+    }
+    const std::string spool = argv[1];
+    double budget_gb = 0, idle_exit = -1;
+    int chunk = 500, max_cases = 0;
+    bool fp64_default = false;
+    for (int a = 2; a < argc; a++) {
+        const std::string k = argv[a];
+        if (k == "--budget-gb" && a + 1 < argc) budget_gb = std::atof(argv[++a]);
+        else if (k == "--chunk" && a + 1 < argc) chunk = std::atoi(argv[++a]);
+        else if (k == "--idle-exit" && a + 1 < argc) idle_exit = std::atof(argv[++a]);
+        else if (k == "--max-cases" && a + 1 < argc) max_cases = std::atoi(argv[++a]);
+        else if (k == "--fp64") fp64_default = true;
+    }
+    itlbm_batch_config cfg{};
+    cfg.hbm_budget = (size_t)(budget_gb * 1e9);
+    cfg.chunk = chunk;
+    cfg.diag_every = 500;
+    cfg.max_cases = max_cases;
+    itlbm_batch *b = nullptr;
+    if (itlbm_batch_create(&cfg, &b) != ITLBM_OK) {
+        std::cerr << "itlbm_batch_create: " << itlbm_last_error() << std::endl;
+        return 2;
+    }
+    std::map<long long, Job> jobs;
+    long long next_tag = 0;
+    std::vector<double> latencies;
+    const double t_start = now_s();
+    double last_work = t_start;
+    long long completed = 0, failed_inputs = 0;
+    std::vector<itlbm_batch_event> ev(1024);
+    while (true) {
+        // new requests
+        for (const std::string &name : list_requests(spool)) {
+            const std::string req = join(spool, name + ".req"), run = join(spool, name + ".run");
+            std::ifstream in(req);
+            std::string dir, prec;
+            in >> dir >> prec;
+            in.close();
+            if (std::rename(req.c_str(), run.c_str()) != 0) continue;
+            Job j;
+            j.name = name;
+            j.dir = dir;
+            std::string err;
+            const bool fp64 = prec == "fp64" || (prec != "fp32" && fp64_default);
+            if (!prepare(j, fp64, err)) {
+                write_text(join(spool, name + ".err"), err + "\n");
+                std::remove(run.c_str());
+                failed_inputs++;
+                continue;
+            }
+            j.t_submit = now_s();
+            const long long tag = next_tag++;
+            if (itlbm_batch_submit(b, &j.desc, j.n_steps, tag) != ITLBM_OK) {
+                write_text(join(spool, name + ".err"), std::string("admission: ") + itlbm_last_error() + "\n");
+                std::remove(run.c_str());
+                failed_inputs++;
+                continue;
+            }
+            jobs.emplace(tag, std::move(j));
+        }
+        itlbm_batch_stats st;
+        itlbm_batch_stats_get(b, &st);
+        if (st.active == 0 && st.pending == 0) {
+            if (idle_exit >= 0 && now_s() - last_work > idle_exit) break;
+            std::this_thread::sleep_for(std::chrono::milliseconds(20));
+            continue;
+        }
+        last_work = now_s();
+        const int r = itlbm_batch_advance(b, nullptr);
+        if (r < 0) {
+            std::cerr << "itlbm_batch_advance: " << itlbm_last_error() << std::endl;
+            break;
+        }
+        int n;
+        while ((n = itlbm_batch_poll(b, ev.data(), (int)ev.size())) > 0) {
+            for (int k = 0; k < n; k++) {
+                const itlbm_batch_event &e = ev[k];
+                auto it = jobs.find(e.tag);
+                if (it == jobs.end()) continue;
+                Job &j = it->second;
+                if (e.kind == ITLBM_EV_DIAG) {
+                    if (j.drop) j.drop->on_diag(e.step, e.drop, nullptr);
+                    else j.stp->on_diag(e.step, e.strip, nullptr);
+                    continue;
+                }
+                const double t = now_s(), latency = t - j.t_submit;
+                const int steps = e.step;
+                const double mlups = latency > 0 ? (double)j.desc.nx * j.desc.ny * steps / (latency * 1e6) : 0;
+                if (j.drop)
+                    j.drop->write_resumo(j.dir, j.desc.op, j.tau, j.beta, j.A, j.nx, j.raio_ini, j.sigma_nominal,
+                                         steps, mlups);
+                else
+                    j.stp->write_resumo(j.dir, j.desc.op, j.tau, j.beta, j.A, j.nx, j.theta, j.sigma_nominal,
+                                        steps, mlups);
+                std::ostringstream done;
+                done << std::setprecision(10) << (e.kind == ITLBM_EV_DONE ? "estavel" : "instavel") << " " << steps
+                     << " " << latency << "\n";
+                write_text(join(spool, j.name + ".done"), done.str());
+                std::remove(join(spool, j.name + ".run").c_str());
+                latencies.push_back(latency);
+                completed++;
+                jobs.erase(it);
+            }
+        }
+        itlbm_batch_stats_get(b, &st);
+        std::ostringstream js;
+        const double wall = now_s() - t_start;
+        js << std::setprecision(10) << "{\"completed\": " << completed << ", \"active\": " << st.active
+           << ", \"pending\": " << st.pending << ", \"invalid\": " << failed_inputs
+           << ", \"p50_s\": " << percentile(latencies, 0.5) << ", \"p99_s\": " << percentile(latencies, 0.99)
+           << ", \"node_updates\": " << st.node_updates << ", \"device_ms\": " << st.device_ms
+           << ", \"wall_s\": " << wall << ", \"mlups_wall\": " << st.node_updates / wall / 1e6
+           << ", \"mlups_device\": " << (st.device_ms > 0 ? st.node_updates / (st.device_ms * 1e3) : 0.0)
+           << ", \"hbm_used\": " << st.hbm_used << "}\n";
+        std::string stats = js.str();
+        for (size_t pos; (pos = stats.find("nan")) != std::string::npos;) stats.replace(pos, 3, "null");
+        write_text(join(spool, "serve_stats.json"), stats);
+    }
+    itlbm_batch_destroy(b);
+    return 0;
+}

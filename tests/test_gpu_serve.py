@@ -1,0 +1,65 @@
+"""Serving: bin/itlbm_serve batches case folders that arrive while others run; bin/itlbm_submit gives
+each request the process contract of Imm_OPS (the way rodar_lote.py runs it).  A case gives the same
+result served in the mix as run alone: in FP64 the served diagnostic files are byte-identical to
+those of bin/itlbm_ops on the same folder."""
+import os
+import subprocess
+import threading
+import time
+from pathlib import Path
+
+import pytest
+
+from test_dropin import BIN, make_case, run
+
+pytestmark = pytest.mark.gpu
+
+
+def submit(d, spool, prec="fp64"):
+    env = dict(os.environ, ITLBM_SPOOL=str(spool), ITLBM_PRECISION=prec, ITLBM_SUBMIT_TIMEOUT="300")
+    return subprocess.run([str(BIN / "itlbm_submit")], cwd=d, capture_output=True, text=True, timeout=400, env=env)
+
+
+def test_served_equals_alone_and_overlaps(tmp_path):
+    spool = tmp_path / "spool"
+    spool.mkdir()
+    server = subprocess.Popen([str(BIN / "itlbm_serve"), str(spool), "--idle-exit", "3", "--chunk", "250"],
+                              stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+    try:
+        cases = [("P3 0.5", 0.225, 40, 1501, None), ("F2", 0.1, 56, 1200, None), ("F3 1.569988", 0.1, 48, 999, None),
+                 ("P1", 0.225, 32, 2001, None), ("P3 2", 0.1, 40, 1001, (2, 1)), ("F1", 0.1, 36, 777, (1, 1))]
+        dirs = [make_case(tmp_path / f"s{k}", op, A, 0.8, nx, steps, pq=pq) for k, (op, A, nx, steps, pq) in
+                enumerate(cases)]
+        results = [None] * len(dirs)
+
+        def go(k, delay):
+            time.sleep(delay)
+            results[k] = submit(dirs[k], spool)
+
+        threads = [threading.Thread(target=go, args=(k, 0.4 * k)) for k in range(len(dirs))]
+        for t in threads:
+            t.start()
+        bad = make_case(tmp_path / "bad", "Z9", 0.1, 0.8, 32, 100)
+        rbad = submit(bad, spool)
+        for t in threads:
+            t.join()
+        assert rbad.returncode == 1 and "operador" in rbad.stderr
+        for k, r in enumerate(results):
+            assert r.returncode == 0, (k, r.stdout, r.stderr)
+            assert "estado = estavel" in r.stdout
+    finally:
+        server.wait(timeout=120)
+    # the same folders run alone by the drop-in programs
+    for k, (op, A, nx, steps, pq) in enumerate(cases):
+        alone = make_case(tmp_path / f"a{k}", op, A, 0.8, nx, steps, pq=pq)
+        prog = "itlbm_incl" if pq else "itlbm_ops"
+        assert run(BIN / prog, alone).returncode == 0
+        names = ["inclinada.dat"] if pq else ["laplace.dat", "iso.dat", "galilean.dat"]
+        for n in names:
+            assert (dirs[k] / n).read_text() == (alone / n).read_text(), (k, n)
+        ra = (dirs[k] / "resumo.dat").read_text().splitlines()
+        rb = (alone / "resumo.dat").read_text().splitlines()
+        assert ra[0] == rb[0] and ra[1].split()[:-1] == rb[1].split()[:-1]  # all but the MLUPS column
+    import json
+    stats = json.loads((spool / "serve_stats.json").read_text())
+    assert stats["completed"] == len(cases) and stats["invalid"] == 1 and stats["p99_s"] > 0

@@ -257,6 +257,19 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #define ITLBM_STEP_MIN_BLOCKS 4
 #endif
 
+// L2 prefetch of this thread's node in the CTA's next tile: the DRAM fetch of tile t + gridDim.x
+// overlaps the work on tile t, which deepens the memory-level parallelism of the persistent CTAs
+// without holding registers.
+template <class S>
+__device__ __forceinline__ void prefetch_tile(const CaseDev &c, int tile, int k) {
+    const int lx = threadIdx.x % TX, ly = threadIdx.x / TX;
+    const int x = (tile % c.tiles_x) * TX + lx, y = (tile / c.tiles_x) * TY + ly;
+    if (x >= c.nx || y >= c.ny) return;
+    const S *src = (const S *)c.buf[(c.parity0 + k) & 1] + (long long)y * c.pitch + x;
+#pragma unroll
+    for (int i = 0; i < 2 * NV; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(src + (long long)i * c.stride));
+}
+
 template <class S>
 __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(const CaseDev *__restrict__ cases,
                                                        const TileRef *__restrict__ tiles,
@@ -268,6 +281,12 @@ __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(co
         const TileRef tr = tiles[t];
         const CaseDev &c = cases[tr.case_id];
         if (k >= c.chunk_len) continue;
+        const int tn = t + gridDim.x;
+        if (tn < nt) {
+            const TileRef trn = tiles[tn];
+            const CaseDev &cn = cases[trn.case_id];
+            if (k < cn.chunk_len) prefetch_tile<S>(cn, trn.tile, k);
+        }
         step_tile<S>(c, tr.tile, k, aux_k, sm);
     }
 }

@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-Default workload ("batch600"): the batched configuration of the north star -- 600 cases drawn from
+Default workload ("batch600"): a batched stream of 600 cases drawn from
 seed 20261203: square boxes with side log-uniform in 64-512, 80 % static drops (R uniform in 10 to
 side/4) and 20 % straight interfaces inclined at atan(q/p), p, q in 1..4; operator uniform over the
 seven; tau uniform in 0.51-2; sigma log-uniform in 0.1-2 (A = 9 sigma / 4 tau for class P); FP32
@@ -111,7 +111,7 @@ def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600):
     upd = st1.node_updates - st0.node_updates
     assert upd == nodes * steps
     b.close()
-    return nodes, ms, allreduce_max(ms, world), (sampler.summary() if sampler else None), len(mix)
+    return nodes, ms, (sampler.summary() if sampler else None), len(mix)
 
 
 def batch_e2e(pkg, steps, n_cases=600):
@@ -144,6 +144,8 @@ def batch_e2e(pkg, steps, n_cases=600):
 
 WORKLOADS = {
     "drop4096": dict(nx=4096, ny=4096, radius=400.0, tipo=3, chi=0.5, xi=1.569988, A=0.225, tau=1.0,
+                     beta=0.8, kprof=2.0 * math.log(9.0) / 3.45),
+    "drop2048": dict(nx=2048, ny=2048, radius=200.0, tipo=3, chi=0.5, xi=1.569988, A=0.225, tau=1.0,
                      beta=0.8, kprof=2.0 * math.log(9.0) / 3.45),
     "drop1024": dict(nx=1024, ny=1024, radius=100.0, tipo=3, chi=0.5, xi=1.569988, A=0.225, tau=1.0,
                      beta=0.8, kprof=2.0 * math.log(9.0) / 3.45),
@@ -195,7 +197,9 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def setup_dist():
+def setup_dist(backend="nccl"):
+    """One process per GPU under torchrun: (world, rank, local rank).  The CPU tests of the replica
+    path use backend "gloo"."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -203,28 +207,36 @@ def setup_dist():
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
-def allreduce_max(v, world):
+def _reduce(v, world, op):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def allreduce_max(v, world):
+    import torch.distributed as dist
+    return _reduce(v, world, dist.ReduceOp.MAX)
 
 
 def allreduce_sum(v, world):
-    if world == 1:
-        return v
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(v, world, dist.ReduceOp.SUM)
+
+
+def replica_mlups(updates, ms, world):
+    """Whole-job MLUPS of N replicas: every rank's node updates over the slowest rank's device time.
+    Returns (mlups, ms_max)."""
+    ms_max = allreduce_max(ms, world)
+    return allreduce_sum(updates, world) / (ms_max * 1e-3) / 1e6, ms_max
 
 
 def barrier(world):
@@ -264,10 +276,9 @@ def device_run(pkg, w, prec, steps, warmup, world, sample_clocks, local):
     barrier(world)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    ms_max = allreduce_max(ms, world)
     n = w["nx"] * w["ny"]
     c.close()
-    return n, ms, ms_max, (sampler.summary() if sampler else None)
+    return n, ms, (sampler.summary() if sampler else None)
 
 
 def e2e_run(pkg, w, prec, steps):
@@ -305,24 +316,55 @@ def cpu_baseline(threads=0):
                       f"{nx}x{nx} drop P3 chi=0.5, {steps} steps, {nthr} OpenMP threads, {dt:.1f} s"}
 
 
+METRIC = "MLUPS & % HBM roofline, batched FP32 vs plain FP64 on 1 B200; p99 case latency"
+REF_SAMPLE = 8  # cases of the batch mix the reference arm steps
+
+
+def batch_config(nodes, ncases, world):
+    return {"workload": "batch600: 600 cases (seed 20261203), side 64-512 log-uniform, 80% drops / 20% "
+                        "inclined strips, 7 operators, tau 0.51-2, sigma 0.1-2, FP32 shifted storage",
+            "nodes": nodes, "cases": ncases,
+            "l2": "state 11+ GB >> 126 MB L2: no flush needed", "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args):
-    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference's own CPU step loop on the host cores, same metric and workload, rank 0 only.
+    Each step is one step of each of the first REF_SAMPLE cases of the batch mix (the reference runs
+    one case per process; a strip steps like a drop of its size and operator -- the step loop does
+    not depend on the initial state)."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import oracle
-    w = WORKLOADS[args.workload]
-    nx = 1024  # bounded sample of the same workload (per-node work is size independent on a CPU)
-    threads = os.cpu_count() or 1
-    total = 0.0
-    tsum = 0.0
-    oracle.time_reference_step(nx, nx, steps=max(1, args.warmup), warmup=0, threads=threads)
-    mlups, dt, nthr = oracle.time_reference_step(nx, nx, steps=args.steps, warmup=0, threads=threads)
-    line = {"impl": "reference", "metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": args.gpus,
+    if args.workload == "batch600":
+        mix = batch_mix()
+        sample = [dict(nx=c["nx"], ny=c["nx"], tipo=c["tipo"], chi=c["chi"], tau=c["tau"], A=c["A"],
+                       radius=c["radius"]) for c in mix[:REF_SAMPLE]]
+        cfg = batch_config(sum(c["nx"] * c["nx"] for c in mix), len(mix), args.gpus)
+        desc = f"first {REF_SAMPLE} cases of the batch mix, sides " + ",".join(str(c["nx"]) for c in sample)
+    else:
+        w = WORKLOADS[args.workload]
+        sample = [dict(nx=1024, ny=1024, tipo=w["tipo"], chi=w["chi"], tau=w["tau"], A=w["A"], radius=100.0)]
+        cfg = {"workload": args.workload, "nodes": w["nx"] * w["ny"], "parallelism": f"replicas x{args.gpus}"}
+        desc = f"1024x1024 sample of {args.workload}"
+    steppers = [oracle.RefStepper(c["nx"], c["ny"], c["tipo"], c["chi"], 1.569988, c["tau"], 0.8, c["A"],
+                                  c["radius"]) for c in sample]
+    for r in steppers:
+        r.step(args.warmup)
+    dt = sum(r.step(args.steps) for r in steppers)
+    upd = sum(r.nodes for r in steppers) * args.steps
+    nthr = steppers[0].threads
+    for r in steppers:
+        r.close()
+    mlups = upd / dt / 1e6
+    cfg["sample"] = desc
+    line = {"impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": args.workload, "sample_nx": nx, "sample_ny": nx},
+            "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": nthr, "kind": "reference",
-                             "sample": f"{nx}x{nx} sample of {args.workload}, {args.steps} steps"},
+                             "sample": f"{desc}; {args.steps} steps each, reference step loop "
+                                       f"(Imm_OPS.cpp:252-287, oracle/_ref, its own flags), {nthr} OpenMP threads"},
             "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -348,23 +390,19 @@ def main():
     torch.cuda.set_device(local)
     import oracle  # noqa: F401  (loads the package binding)
     pkg = oracle.load_package()
-    w = WORKLOADS[args.workload]
     peak, peak_kind = hbm_peak()
 
     single = WORKLOADS["drop4096" if args.workload == "batch600" else args.workload]
     if args.workload == "batch600":
-        nodes, ms, ms_max, clocks, ncases = batch_run(pkg, args.steps, args.warmup, world, rank == 0, local)
-        mlups = allreduce_sum(nodes * args.steps, world) / (ms_max * 1e-3) / 1e6
+        nodes, ms, clocks, ncases = batch_run(pkg, args.steps, args.warmup, world, rank == 0, local)
+        mlups, ms_max = replica_mlups(nodes * args.steps, ms, world)
         achieved = 304.0 * nodes * args.steps / (ms * 1e-3) / 1e9
         launches = 2 * args.steps  # one FP64 and one FP32 persistent launch per step (no FP64 cases here)
-        cfg = {"workload": "batch600: 600 cases (seed 20261203), side 64-512 log-uniform, 80% drops / 20% "
-                           "inclined strips, 7 operators, tau 0.51-2, sigma 0.1-2, FP32 shifted storage",
-               "nodes": nodes, "cases": ncases,
-               "l2": "state 11+ GB >> 126 MB L2: no flush needed", "parallelism": f"replicas x{world}"}
+        cfg = batch_config(nodes, ncases, world)
     else:
-        nodes, ms, ms_max, clocks = device_run(pkg, single, pkg.PREC_F32, args.steps, args.warmup, world,
-                                               rank == 0, local)
-        mlups = allreduce_sum(nodes * args.steps, world) / (ms_max * 1e-3) / 1e6
+        nodes, ms, clocks = device_run(pkg, single, pkg.PREC_F32, args.steps, args.warmup, world,
+                                       rank == 0, local)
+        mlups, ms_max = replica_mlups(nodes * args.steps, ms, world)
         achieved = 304.0 * nodes * args.steps / (ms * 1e-3) / 1e9
         launches = args.steps
         cfg = {"workload": f"{args.workload}: {single['nx']}x{single['ny']}x1 static drop, P3 chi=0.5, FP32",
@@ -372,11 +410,11 @@ def main():
 
     # the single 4096^2 case, FP32 and plain FP64
     ks = max(50, args.steps // 2)
-    n1, ms1, ms1_max, _ = device_run(pkg, single, pkg.PREC_F32, ks, args.warmup, world, False, local)
-    n64, ms64, ms64_max, _ = device_run(pkg, single, pkg.PREC_F64, ks, args.warmup, world, False, local)
-    single32 = {"value": allreduce_sum(n1 * ks, world) / (ms1_max * 1e-3) / 1e6, "unit": "MLUPS", "steps": ks,
+    n1, ms1, _ = device_run(pkg, single, pkg.PREC_F32, ks, args.warmup, world, False, local)
+    n64, ms64, _ = device_run(pkg, single, pkg.PREC_F64, ks, args.warmup, world, False, local)
+    single32 = {"value": replica_mlups(n1 * ks, ms1, world)[0], "unit": "MLUPS", "steps": ks,
                 "roofline_frac": 304.0 * n1 * ks / (ms1 * 1e-3) / 1e9 / peak}
-    fp64 = {"value": allreduce_sum(n64 * ks, world) / (ms64_max * 1e-3) / 1e6, "unit": "MLUPS", "steps": ks,
+    fp64 = {"value": replica_mlups(n64 * ks, ms64, world)[0], "unit": "MLUPS", "steps": ks,
             "roofline_frac": 608.0 * n64 * ks / (ms64 * 1e-3) / 1e9 / peak,
             "workload": "4096x4096x1 static drop R=400, P3 chi=0.5, FP64 plain (bit-identical to the reference)"}
 
@@ -391,7 +429,7 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": "MLUPS & % HBM roofline, batched FP32 vs plain FP64 on 1 B200; p99 case latency",
+            "metric": METRIC,
             "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,

@@ -194,7 +194,7 @@ typedef struct itlbm_batch_config {
     int    max_cases;         /* slots; 0 = 4096                                                  */
     int    chunk;             /* steps per graph replay; 0 = 500 (PASSOS_DIAG)                    */
     int    diag_every;        /* diagnostic interval; 0 = 500                                     */
-    int    ctas_per_sm;       /* persistent CTAs per SM; 0 = from the occupancy of the kernels    */
+    int    ctas_per_sm;       /* 0 = one CTA per tile; > 0 = that many persistent CTAs per SM      */
 } itlbm_batch_config;
 
 enum { ITLBM_EV_DIAG = 0, ITLBM_EV_DONE = 1, ITLBM_EV_UNSTABLE = 2 };

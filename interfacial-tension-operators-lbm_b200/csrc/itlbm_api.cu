@@ -91,7 +91,6 @@ struct itlbm_case {
     long long steps = 0;
     int aux_valid = 0;
     int device = 0;
-    int grid = 0;  // persistent CTAs of the step launches
 };
 
 extern "C" {
@@ -268,17 +267,10 @@ int itlbm_case_step(itlbm_case *c, int nsteps, int flags, void *stream) {
     }
     cudaStream_t s = (cudaStream_t)stream;
     if (c->steps + nsteps > (long long)INT_MAX - 2) return fail(ITLBM_E_STATE, "step counter overflow");
-    // persistent CTAs: as many as are resident, each striding over the tiles (and prefetching its
-    // next tile into L2)
-    if (c->grid == 0) {
-        int sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-        c->grid = std::min(c->ntiles, std::max(1, step_occupancy(c->host.prec)) * sms);
-    }
     for (int i = 0; i < nsteps; i++) {
         const int k = (int)(c->steps + i);
         const int aux_k = (keep && i == nsteps - 1) ? k : -1;
-        cudaError_t e = launch_step(c->dev, c->tiles, c->ntiles, nullptr, c->grid, k, aux_k,
+        cudaError_t e = launch_step(c->dev, c->tiles, c->ntiles, nullptr, c->ntiles, k, aux_k,
                                     c->host.prec, s);
         if (e != cudaSuccess) return cuda_fail(e, "step kernel");
     }

@@ -125,6 +125,8 @@ int upload_tables(itlbm_batch *b) {
             if (e != cudaSuccess) return cuda_fail(e, "work table upload");
         }
     }
+    if (b->cfg.ctas_per_sm <= 0)
+        for (int p = 0; p < 2; p++) b->grid[p] = n[p];
     // the graph reads the table pointers it was captured with: keep them, or re-capture
     cudaError_t e = cudaMemcpyAsync(b->d_ntiles, n, sizeof(int) * 2, cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "work table length");
@@ -237,10 +239,10 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
         cudaMemGetInfo(&fr, &tot);
         b->cfg.hbm_budget = (size_t)(0.9 * (double)fr);
     }
-    for (int p = 0; p < 2; p++) {
-        const int occ = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm : step_occupancy(p == 0 ? ITLBM_PREC_F64 : ITLBM_PREC_F32);
-        b->grid[p] = std::max(1, occ) * b->sms;
-    }
+    // launch shape: one CTA per tile of the work table (the grid follows the table and the graph is
+    // re-captured when it changes), or, with ctas_per_sm > 0, that many persistent CTAs per SM
+    // striding over the table
+    for (int p = 0; p < 2; p++) b->grid[p] = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm * b->sms : 0;
     const int M = b->cfg.max_cases;
     b->slots.assign(M, nullptr);
     for (int s = M - 1; s >= 0; s--) b->free_slots.push_back(s);
@@ -344,9 +346,10 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
     if (e != cudaSuccess) return cuda_fail(e, "case table upload");
     if (b->tables_dirty) {
         TileRef *old0 = b->d_tiles[0], *old1 = b->d_tiles[1];
+        const int g0 = b->grid[0], g1 = b->grid[1];
         r = upload_tables(b);
         if (r) return r;
-        if (old0 != b->d_tiles[0] || old1 != b->d_tiles[1]) {
+        if (old0 != b->d_tiles[0] || old1 != b->d_tiles[1] || g0 != b->grid[0] || g1 != b->grid[1]) {
             r = capture_graph(b);
             if (r) return r;
         }

@@ -233,9 +233,9 @@ __device__ __forceinline__ void colisao_site_f64(double (&fR)[NV], double (&fB)[
 // ---------------------------------------------------------------------------------------------
 // Recolouring split of the FP32 form: d_i = rho^N f_i - fat2 w_i cos(phi_i) with
 // fat2 = 2 beta c_R c_B rho = beta (1 - rho^N^2) rho / 2 (c_R - c_B = rho^N); d_0 is the complement
-// D - sum_{i>=1} d_i (see collide_f32).
+// D - sum_{i>=1} d_i, formed by the step kernel with FP64 sums.
 struct Recolour32 {
-    float D, phi, fat2, gx, gy, gz, inv_mod;
+    float phi, fat2, gx, gy, gz, inv_mod;
     bool skip;
 };
 
@@ -324,7 +324,6 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
         sfor<1, NV>([&](auto I) { s += e[decltype(I)::value]; });
         e[0] = drho - s;
     }
-    rc.D = D;
     rc.phi = phi;
     rc.fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
     rc.inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;

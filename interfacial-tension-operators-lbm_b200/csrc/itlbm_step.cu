@@ -92,6 +92,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     const int x = x0 + lx, y = y0 + ly;
     const bool valid = (x < xe) && (y < ye);
     S f[NV], sa = S(0), sb = S(0);
+    double sbd = 0.0;
     if (x < xe + H && y < ye + H) {
         const int xw = valid ? x : wrapi(x, nx), yw = valid ? y : wrapi(y, ny);
         const long long off = (long long)yw * pitch + xw;
@@ -102,8 +103,15 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         for (int i = 0; i < NV; i++) b[i] = __ldg(src + (long long)(NV + i) * stride + off);
 #pragma unroll
         for (int i = 0; i < NV; i++) sa = sa + a[i];
+        if constexpr (std::is_same<S, float>::value) {
+            // FP32: the colour difference D = sum d_i in FP64 (see the split below)
 #pragma unroll
-        for (int i = 0; i < NV; i++) sb = sb + b[i];
+            for (int i = 0; i < NV; i++) sbd += (double)b[i];
+            sb = (float)sbd;
+        } else {
+#pragma unroll
+            for (int i = 0; i < NV; i++) sb = sb + b[i];
+        }
         if constexpr (std::is_same<S, double>::value) {
 #pragma unroll
             for (int i = 0; i < NV; i++) f[i] = a[i] + b[i];
@@ -212,19 +220,23 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             else collide_f32<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
             skip = rc.skip;
             if (!skip) {
+                // d_0 is the complement of the moving d_i against the incoming D, both summed in
+                // FP64: the d_i are O(w_i rho), so FP32 sums would round by ~1e-8 rho per node and
+                // step, coherently over uniform regions, and drift the colour masses (1e-6 in 2000
+                // steps); in FP64 the only rounding left is that of d_0 itself.
                 const float rho0 = (float)c.rho0;
-                float dsum = 0.f;
+                double dsum = 0.0;
                 sfor<1, NV>([&](auto I) {
                     constexpr int i = decltype(I)::value;
                     const long long o = dst_off(i);
                     const float d = split32<i>(rc, f[i], rho0);
-                    dsum += d;
+                    dsum += (double)d;
                     dst[(long long)i * stride + o] = f[i];
                     dst[(long long)(NV + i) * stride + o] = d;
                 });
                 const long long o0 = dst_off(0);
                 dst[o0] = f[0];
-                dst[(long long)NV * stride + o0] = rc.D - dsum;
+                dst[(long long)NV * stride + o0] = (float)(sbd - dsum);
             }
         }
         if (skip) {  // rho <= 1e-30: the site is streamed unchanged (Operadores_tensao.cpp:347)
@@ -257,19 +269,6 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #define ITLBM_STEP_MIN_BLOCKS 4
 #endif
 
-// L2 prefetch of this thread's node in the CTA's next tile: the DRAM fetch of tile t + gridDim.x
-// overlaps the work on tile t, which deepens the memory-level parallelism of the persistent CTAs
-// without holding registers.
-template <class S>
-__device__ __forceinline__ void prefetch_tile(const CaseDev &c, int tile, int k) {
-    const int lx = threadIdx.x % TX, ly = threadIdx.x / TX;
-    const int x = (tile % c.tiles_x) * TX + lx, y = (tile / c.tiles_x) * TY + ly;
-    if (x >= c.nx || y >= c.ny) return;
-    const S *src = (const S *)c.buf[(c.parity0 + k) & 1] + (long long)y * c.pitch + x;
-#pragma unroll
-    for (int i = 0; i < 2 * NV; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(src + (long long)i * c.stride));
-}
-
 template <class S>
 __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(const CaseDev *__restrict__ cases,
                                                        const TileRef *__restrict__ tiles,
@@ -281,12 +280,6 @@ __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(co
         const TileRef tr = tiles[t];
         const CaseDev &c = cases[tr.case_id];
         if (k >= c.chunk_len) continue;
-        const int tn = t + gridDim.x;
-        if (tn < nt) {
-            const TileRef trn = tiles[tn];
-            const CaseDev &cn = cases[trn.case_id];
-            if (k < cn.chunk_len) prefetch_tile<S>(cn, trn.tile, k);
-        }
         step_tile<S>(c, tr.tile, k, aux_k, sm);
     }
 }

@@ -290,23 +290,45 @@ class RefStrip:
             pass
 
 
+class RefStepper:
+    """The reference's own step loop (Imm_OPS.cpp:252-287) on one drop case, through
+    oracle/_ref/libref_ops_fast.so (built from the reference's sources with its own flags), run on
+    `threads` host threads (0 = all cores).  A CPU baseline, never a product path."""
+
+    def __init__(self, nx, ny, tipo=3, chi=0.5, xi=1.569988, tau=1.0, beta=0.8, A=0.225, radius=0.0,
+                 threads=0):
+        import os
+        L = C.CDLL(str(REF_DIR / "libref_ops_fast.so"))
+        vp, d, i = C.c_void_p, C.c_double, C.c_int
+        L.ref_ops_create.restype, L.ref_ops_create.argtypes = vp, [i, i, i, d, d, d, d, d, d, d, d, d, d, i]
+        L.ref_ops_step.restype, L.ref_ops_step.argtypes = None, [vp, i]
+        L.ref_ops_destroy.restype, L.ref_ops_destroy.argtypes = None, [vp]
+        self._L = L
+        self.threads = threads if threads > 0 else (os.cpu_count() or 1)
+        self.nodes = nx * ny
+        radius = radius if radius > 0 else 0.25 * nx
+        self._h = L.ref_ops_create(nx, ny, tipo, chi, xi, tau, beta, A, radius, K_PERFIL, 0.0, 1.0, 1.0,
+                                   self.threads)
+
+    def step(self, n):
+        """n steps; returns the wall time in seconds."""
+        import time
+        t0 = time.perf_counter()
+        self._L.ref_ops_step(self._h, n)
+        return time.perf_counter() - t0
+
+    def close(self):
+        if self._h:
+            self._L.ref_ops_destroy(self._h)
+            self._h = None
+
+
 def time_reference_step(nx, ny, tipo=3, chi=0.5, xi=1.569988, tau=1.0, beta=0.8, A=0.225, radius=0.0,
                         steps=10, warmup=1, threads=0):
-    """Time the reference's own step loop (Imm_OPS.cpp:252-287 via oracle/_ref/libref_ops_fast.so,
-    built with the reference's flags) on the host cores.  Returns (MLUPS, seconds, threads used)."""
-    import os
-    import time
-    L = C.CDLL(str(REF_DIR / "libref_ops_fast.so"))
-    vp, d, i = C.c_void_p, C.c_double, C.c_int
-    L.ref_ops_create.restype, L.ref_ops_create.argtypes = vp, [i, i, i, d, d, d, d, d, d, d, d, d, d, i]
-    L.ref_ops_step.restype, L.ref_ops_step.argtypes = None, [vp, i]
-    L.ref_ops_destroy.restype, L.ref_ops_destroy.argtypes = None, [vp]
-    nthr = threads if threads > 0 else (os.cpu_count() or 1)
-    radius = radius if radius > 0 else 0.25 * nx
-    h = L.ref_ops_create(nx, ny, tipo, chi, xi, tau, beta, A, radius, K_PERFIL, 0.0, 1.0, 1.0, nthr)
-    L.ref_ops_step(h, warmup)
-    t0 = time.perf_counter()
-    L.ref_ops_step(h, steps)
-    dt = time.perf_counter() - t0
-    L.ref_ops_destroy(h)
-    return nx * ny * steps / dt / 1e6, dt, nthr
+    """Time the reference's own step loop on the host cores.  Returns (MLUPS, seconds, threads)."""
+    r = RefStepper(nx, ny, tipo, chi, xi, tau, beta, A, radius, threads)
+    if warmup:
+        r.step(warmup)
+    dt = r.step(steps)
+    r.close()
+    return nx * ny * steps / dt / 1e6, dt, r.threads

@@ -2,7 +2,7 @@
 with strict IEEE semantics, see test_oracle_pin.py).
 
 The FP64 plain path is compared BIT FOR BIT: initial state, populations at the top of each step,
-post-collision populations and the class-F force.  The bar of the north-star (max |df| <= 1e-12
+post-collision populations and the class-F force.  The FP64 accuracy bar (max |df| <= 1e-12
 after 1000 steps) is therefore met with max |df| = 0.  Diagnostics reduce in a different order on
 the device, so they are compared with a relative tolerance of 1e-10 (absolute floor for quantities
 that are zero up to round-off).
@@ -282,8 +282,9 @@ def test_fp32_one_step(gpu, name, tipo, chi, xi, A):
 
 @pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=OP_IDS)
 def test_fp32_tracks_fp64(gpu, name, tipo, chi, xi, A):
-    """North-star accuracy of the FP32 storage after 2000 steps: Laplace pressure jump within 0.5 %
-    and peak spurious velocity within 5 % of FP64; colour masses conserved."""
+    """Accuracy bar of the FP32 storage after 2000 steps: Laplace pressure jump within 0.5 %
+    and peak spurious velocity within 5 % of FP64; colour masses conserved to 2e-7 (the rounding of
+    the rest population d_0, the only one left in the FP32 update of the colour difference)."""
     nx = 80
     c64 = gpu_case(gpu, nx, nx, tipo, chi, xi, A, tau=0.8, radius=16.0)
     c32 = gpu_case(gpu, nx, nx, tipo, chi, xi, A, tau=0.8, radius=16.0, prec=1)
@@ -298,7 +299,7 @@ def test_fp32_tracks_fp64(gpu, name, tipo, chi, xi, A):
           f"R {d32.raio / d64.raio - 1:+.2e}  mass_R {m1[0] / m0[0] - 1:+.2e}")
     assert abs(d32.delta_p - d64.delta_p) <= 5e-3 * abs(d64.delta_p)
     assert abs(d32.u_max - d64.u_max) <= 0.05 * d64.u_max
-    assert abs(m1[0] - m0[0]) <= 1e-6 * m0[0] and abs(m1[1] - m0[1]) <= 1e-6 * m0[1]
+    assert abs(m1[0] - m0[0]) <= 2e-7 * m0[0] and abs(m1[1] - m0[1]) <= 2e-7 * m0[1]
     assert abs(d32.raio - d64.raio) <= 2e-4 * d64.raio
     c64.close()
     c32.close()

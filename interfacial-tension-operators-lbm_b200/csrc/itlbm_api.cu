@@ -321,6 +321,43 @@ int itlbm_case_diag_drop(itlbm_case *c, int step, double x_ini, double y_ini, it
     return ITLBM_OK;
 }
 
+// The same kernels as itlbm_case_diag_drop on a fixed device scratch; no allocation of any kind.
+int itlbm_case_diag_drop_static(itlbm_case *c, int step, double x_ini, double y_ini,
+                                itlbm_drop_diag *out, void *stream) {
+    if (!c || !out) return fail(ITLBM_E_ARG, "NULL argument");
+    const int nx = c->host.nx, ny = c->host.ny;
+    if (nx > ITLBM_STATIC_DIAG_MAX_SIDE || ny > ITLBM_STATIC_DIAG_MAX_SIDE ||
+        (long long)nx * ny > ITLBM_STATIC_DIAG_MAX_NODES)
+        return fail(ITLBM_E_ARG, "itlbm_case_diag_drop_static: case of " + std::to_string(nx) + " x " +
+                                     std::to_string(ny) + " nodes is larger than the static scratch (at most " +
+                                     std::to_string(ITLBM_STATIC_DIAG_MAX_NODES) + " nodes, sides up to " +
+                                     std::to_string(ITLBM_STATIC_DIAG_MAX_SIDE) +
+                                     "); use itlbm_case_diag_drop");
+    if (c->steps < 1) return fail(ITLBM_E_STATE, "no step has run yet");
+    const bool force = c->host.tipo >= ITLBM_OP_F1;
+    if (force && !c->aux_valid)
+        return fail(ITLBM_E_STATE, "class F: the last step must keep aux (ITLBM_STEP_KEEP_AUX)");
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    void *base = nullptr;
+    size_t bytes = 0;
+    if ((e = static_diag_scratch(c->device, &base, &bytes)) != cudaSuccess)
+        return cuda_fail(e, "cudaGetSymbolAddress(static diagnostic scratch)");
+    DiagScratch s;
+    if ((e = diag_bind(s, base, bytes, nx, ny)) != cudaSuccess)
+        return fail(ITLBM_E_ARG, "itlbm_case_diag_drop_static: case does not fit the static scratch");
+    cudaStream_t st = (cudaStream_t)stream;
+    itlbm_drop_diag *od = (itlbm_drop_diag *)s.out;
+    e = launch_diag_drop(c->dev, c->host, s, (int)(c->steps & 1), step, c->desc.v0, x_ini, y_ini, force,
+                         od, st);
+    if (e != cudaSuccess) return cuda_fail(e, "diagnostic kernels");
+    if ((e = cudaMemcpyAsync(out, od, sizeof(itlbm_drop_diag), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_fail(e, "diagnostic copy");
+    out->step = step;
+    return ITLBM_OK;
+}
+
 int itlbm_case_diag_strip(itlbm_case *c, int step, itlbm_strip_diag *out, void *stream) {
     if (!c || !out) return fail(ITLBM_E_ARG, "NULL argument");
     if (c->desc.geometry != ITLBM_GEOM_STRIP) return fail(ITLBM_E_STATE, "not a strip case");

@@ -860,6 +860,38 @@ cudaError_t diag_alloc(DiagScratch &s, int nx, int ny) {
     return cudaSuccess;
 }
 
+namespace {
+size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
+int nshell_for(int nx, int ny) { return (int)(sqrt((double)(nx * nx + ny * ny + 1)) / 0.5) + 2; }
+}  // namespace
+
+size_t diag_bytes(int nx, int ny) {
+    const size_t n = (size_t)nx * ny;
+    return up256(sizeof(double) * 6 * n) + up256(sizeof(double) * 32 * (size_t)MAXB) +
+           up256(sizeof(long long) * 2 * (size_t)nshell_for(nx, ny)) +
+           up256(sizeof(DropState) + sizeof(StripState) + 64) +
+           up256(sizeof(itlbm_drop_diag) + sizeof(itlbm_strip_diag) + 64);
+}
+
+cudaError_t diag_bind(DiagScratch &s, void *base, size_t bytes, int nx, int ny) {
+    if (!base || ((uintptr_t)base & 255) || diag_bytes(nx, ny) > bytes) return cudaErrorInvalidValue;
+    const int n = nx * ny;
+    char *p = (char *)base;
+    s.n = n;
+    s.nblocks = nblocks_for(n);
+    s.nshell = nshell_for(nx, ny);
+    s.node = (double *)p;
+    p += up256(sizeof(double) * 6 * (size_t)n);
+    s.part = (double *)p;
+    p += up256(sizeof(double) * 32 * (size_t)MAXB);
+    s.shell = (long long *)p;
+    p += up256(sizeof(long long) * 2 * (size_t)s.nshell);
+    s.state = (double *)p;
+    p += up256(sizeof(DropState) + sizeof(StripState) + 64);
+    s.out = p;
+    return cudaSuccess;
+}
+
 void diag_free(DiagScratch &s) {
     if (s.node) cudaFree(s.node);
     if (s.part) cudaFree(s.part);

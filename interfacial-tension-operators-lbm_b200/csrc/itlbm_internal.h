@@ -116,6 +116,14 @@ struct DiagScratch {
 };
 cudaError_t diag_alloc(DiagScratch &s, int nx, int ny);
 void diag_free(DiagScratch &s);
+// Bytes of one diagnostic scratch for an nx x ny case, and the same scratch laid out in a block the
+// caller already holds (256-byte aligned, at least diag_bytes long); diag_bind allocates nothing and
+// the block stays the caller's (never pass a bound scratch to diag_free).
+size_t diag_bytes(int nx, int ny);
+cudaError_t diag_bind(DiagScratch &s, void *base, size_t bytes, int nx, int ny);
+// The static scratch of itlbm_case_diag_drop_static on the current device: its address (looked up
+// once per device) and its size in bytes.
+cudaError_t static_diag_scratch(int device, void **base, size_t *bytes);
 cudaError_t launch_diag_drop(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
                              int step, double v0, double x_ini, double y_ini, bool use_force,
                              itlbm_drop_diag *out_dev, cudaStream_t st);

@@ -57,11 +57,37 @@ void fill_params(CaseDev &c, const itlbm_operador &op, double tau, double A_fact
 }
 
 cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                        const int *ntiles_dev, int grid, int k, int aux_k, int prec,
+                        const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
                         cudaStream_t s) {
-    return prec == ITLBM_PREC_F64
-               ? launch_step_f64(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s)
-               : launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
+    if (prec == ITLBM_PREC_F64) return launch_step_f64(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
+    return march ? launch_march_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s)
+                 : launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
+}
+
+bool march_default() {
+    const char *v = getenv("ITLBM_STEP_KERNEL");
+    return !(v && std::strcmp(v, "tile") == 0);
+}
+
+void case_layout(CaseDev &h, int nx, int ny, int prec, bool march) {
+    h.nx = nx;
+    h.ny = ny;
+    h.pitch = (nx + 31) / 32 * 32;
+    h.stride = (long long)h.pitch * ny;
+    h.tiles_x = (nx + TX - 1) / TX;
+    h.tiles = h.tiles_x * ((ny + TY - 1) / TY);
+    h.prec = prec;
+    h.march = (prec == ITLBM_PREC_F32 && march) ? 1 : 0;
+    h.m_strips = (nx + MARCH_W - 1) / MARCH_W;
+    h.m_items = h.m_strips * ((ny + MARCH_SEG - 1) / MARCH_SEG);
+}
+
+int case_items(const CaseDev &h) { return h.march ? h.m_items : h.tiles; }
+
+cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf) {
+    h.buf[0] = mem;
+    h.buf[1] = (char *)mem + per_buf;
+    return h.march ? encode_state_map(h, mem, per_buf) : cudaSuccess;
 }
 
 int step_occupancy(int prec) {
@@ -201,14 +227,7 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
     c->desc = *d;
     c->device = dev;
     CaseDev &h = c->host;
-    h.nx = d->nx;
-    h.ny = d->ny;
-    h.pitch = (d->nx + 31) / 32 * 32;
-    h.stride = (long long)h.pitch * d->ny;
-    h.tiles_x = (d->nx + TX - 1) / TX;
-    const int tiles_y = (d->ny + TY - 1) / TY;
-    h.tiles = h.tiles_x * tiles_y;
-    h.prec = d->precision;
+    case_layout(h, d->nx, d->ny, d->precision, march_default());
     h.parity0 = 0;
     h.chunk_len = INT_MAX;
     h.aux_at_end = 0;
@@ -219,10 +238,13 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
         itlbm_case_destroy(c);
         return cuda_fail(e, "cudaMalloc(state)");
     }
-    h.buf[0] = c->mem;
-    h.buf[1] = (char *)c->mem + per_buf;
+    if ((e = case_bind(h, c->mem, per_buf)) != cudaSuccess ||
+        (h.march && (e = march_prepare()) != cudaSuccess)) {
+        itlbm_case_destroy(c);
+        return cuda_fail(e, "state tensor map");
+    }
     h.aux = nullptr;
-    c->ntiles = h.tiles;
+    c->ntiles = case_items(h);
     std::vector<TileRef> tl(c->ntiles);
     for (int t = 0; t < c->ntiles; t++) tl[t] = TileRef{0, t};
     if ((e = cudaMalloc(&c->tiles, sizeof(TileRef) * c->ntiles)) != cudaSuccess ||
@@ -252,6 +274,8 @@ static int ensure_aux(itlbm_case *c) {
     cudaMemset(c->aux, 0, sizeof(double) * 4 * (size_t)c->host.stride);
     c->host.aux = c->aux;
     e = cudaMemcpy(c->dev, &c->host, sizeof(CaseDev), cudaMemcpyHostToDevice);
+    // a pageable copy may return before the data lands, and the steps may go to a non-blocking stream
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(case)");
     return ITLBM_OK;
 }
@@ -271,7 +295,7 @@ int itlbm_case_step(itlbm_case *c, int nsteps, int flags, void *stream) {
         const int k = (int)(c->steps + i);
         const int aux_k = (keep && i == nsteps - 1) ? k : -1;
         cudaError_t e = launch_step(c->dev, c->tiles, c->ntiles, nullptr, c->ntiles, k, aux_k,
-                                    c->host.prec, s);
+                                    c->host.prec, c->host.march != 0, s);
         if (e != cudaSuccess) return cuda_fail(e, "step kernel");
     }
     c->steps += nsteps;
@@ -283,7 +307,9 @@ int itlbm_case_sync(itlbm_case *c) {
     if (!c) return fail(ITLBM_E_ARG, "NULL case");
     cudaSetDevice(c->device);
     cudaError_t e = cudaDeviceSynchronize();
-    return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "synchronize");
+    if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+    if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
+    return ITLBM_OK;
 }
 
 long long itlbm_case_steps_done(const itlbm_case *c) { return c ? c->steps : -1; }
@@ -398,7 +424,8 @@ int itlbm_case_read_pops(itlbm_case *c, int which, double *fR, double *fB) {
     if (r) return r;
     const size_t n = (size_t)c->host.nx * c->host.ny;
     const int cur = (int)(c->steps & 1);
-    cudaError_t e = launch_export(c->dev, c->host.nx, c->host.ny, cur, which, c->tmp, c->tmp + NV * n, 0);
+    cudaError_t e = cudaDeviceSynchronize();  // steps may have gone to another stream
+    if (e == cudaSuccess) e = launch_export(c->dev, c->host.nx, c->host.ny, cur, which, c->tmp, c->tmp + NV * n, 0);
     if (e == cudaSuccess) e = cudaMemcpy(fR, c->tmp, sizeof(double) * NV * n, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(fB, c->tmp + NV * n, sizeof(double) * NV * n, cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "read_pops");
@@ -432,8 +459,9 @@ int itlbm_case_read_fields(itlbm_case *c, double *rho_R, double *rho_B, double *
     if (r) return r;
     const size_t n = (size_t)c->host.nx * c->host.ny;
     double *t = c->tmp;
-    cudaError_t e = launch_fields(c->dev, c->host, (int)(c->steps & 1), cls_f, t, t + n, t + 2 * n,
-                                  t + 3 * n, t + 4 * n, 0);
+    cudaError_t e = cudaDeviceSynchronize();  // steps may have gone to another stream
+    if (e == cudaSuccess)
+        e = launch_fields(c->dev, c->host, (int)(c->steps & 1), cls_f, t, t + n, t + 2 * n, t + 3 * n, t + 4 * n, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     double *outs[5] = {rho_R, rho_B, ux, uy, uz};
     for (int k = 0; k < 5 && e == cudaSuccess; k++)

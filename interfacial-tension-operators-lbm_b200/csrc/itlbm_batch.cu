@@ -80,6 +80,7 @@ struct itlbm_batch {
     int *d_ntiles = nullptr;
     bool tables_dirty = true;
     int grid[2] = {0, 0};
+    bool march = true;  // FP32 cases run the marching kernel
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DiagScratch diag;
@@ -108,7 +109,8 @@ int upload_tables(itlbm_batch *b) {
         if (!a) continue;
         const CaseDev &c = b->h_cases[a->slot];
         const int p = a->desc.precision == ITLBM_PREC_F64 ? 0 : 1;
-        for (int k = 0; k < c.tiles; k++) t[p].push_back(TileRef{a->slot, k});
+        const int n = case_items(c);
+        for (int k = 0; k < n; k++) t[p].push_back(TileRef{a->slot, k});
     }
     int n[2];
     for (int p = 0; p < 2; p++) {
@@ -142,8 +144,8 @@ int capture_graph(itlbm_batch *b) {
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "begin capture");
     for (int k = 0; k < b->cfg.chunk; k++) {
-        launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, b->stream);
-        launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->stream);
+        launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, false, b->stream);
+        launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->march, b->stream);
     }
     e = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) return cuda_fail(e, "end capture");
@@ -178,13 +180,7 @@ int admit(itlbm_batch *b) {
         a->bytes = bytes;
         const itlbm_case_desc &d = p.desc;
         CaseDev h{};
-        h.nx = d.nx;
-        h.ny = d.ny;
-        h.pitch = (d.nx + 31) / 32 * 32;
-        h.stride = (long long)h.pitch * d.ny;
-        h.tiles_x = (d.nx + TX - 1) / TX;
-        h.tiles = h.tiles_x * ((d.ny + TY - 1) / TY);
-        h.prec = d.precision;
+        case_layout(h, d.nx, d.ny, d.precision, b->march);
         fill_params(h, d.op, d.tau, d.A_fact, d.beta, d.rho_B > 0 ? d.rho_B : 1.0);
         const size_t elem = d.precision == ITLBM_PREC_F64 ? 8 : 4;
         const size_t per_buf = (size_t)2 * NV * h.stride * elem;
@@ -196,8 +192,12 @@ int admit(itlbm_batch *b) {
             cudaGetLastError();
             return ITLBM_OK;  // the device is fuller than the budget says: try again next round
         }
-        h.buf[0] = a->mem;
-        h.buf[1] = (char *)a->mem + per_buf;
+        if ((e = case_bind(h, a->mem, per_buf)) != cudaSuccess) {
+            cudaFree(a->mem);
+            if (a->aux) cudaFree(a->aux);
+            delete a;
+            return cuda_fail(e, "state tensor map");
+        }
         h.aux = a->aux;
         h.parity0 = 0;
         h.chunk_len = 0;
@@ -206,7 +206,8 @@ int admit(itlbm_batch *b) {
         a->slot = slot;
         b->slots[slot] = a;
         b->h_cases[slot] = h;
-        e = cudaMemcpy(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice);
+        // on the batch stream, which is not ordered after the legacy stream's copies
+        e = cudaMemcpyAsync(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream);
         if (e == cudaSuccess) e = launch_init(h, b->d_cases + slot, d, b->stream);
         if (e != cudaSuccess) return cuda_fail(e, "admission");
         b->hbm_used += bytes;
@@ -234,6 +235,11 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
         return cuda_fail(e, "cudaGetDevice");
     }
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    b->march = march_default();
+    if (b->march && (e = march_prepare()) != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "marching kernel attributes");
+    }
     if (b->cfg.hbm_budget == 0) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
@@ -257,8 +263,9 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
         itlbm_batch_destroy(b);
         return cuda_fail(e, "batch allocation");
     }
-    cudaMemset(b->d_cases, 0, sizeof(CaseDev) * M);
-    cudaMemset(b->d_ntiles, 0, sizeof(int) * 2);
+    cudaMemsetAsync(b->d_cases, 0, sizeof(CaseDev) * M, b->stream);
+    cudaMemsetAsync(b->d_ntiles, 0, sizeof(int) * 2, b->stream);
+    cudaStreamSynchronize(b->stream);
     // work tables with room for a first batch, so the graph can be captured with their addresses
     for (int p = 0; p < 2; p++) {
         b->tiles_cap[p] = 1 << 16;
@@ -361,8 +368,8 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         if (e != cudaSuccess) return cuda_fail(e, "graph launch");
     } else {
         for (int k = 0; k < K; k++) {
-            launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, b->stream);
-            launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->stream);
+            launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, false, b->stream);
+            launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->march, b->stream);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "step launches");
     }
@@ -403,6 +410,7 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         measured.push_back(a);
     }
     if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "replay");
+    if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
     float ms = 0;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->device_ms += ms;

@@ -1,6 +1,7 @@
 // itlbm_internal.h -- definitions shared by the CUDA translation units of libitlbm.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -23,6 +24,9 @@ constexpr int PY = TY + 2 * HMAX;  // staged phase tile height
 constexpr int QX = TX + 2;         // ring-1 region of the F1/F2 auxiliary fields
 constexpr int QY = TY + 2;
 constexpr int STEP_THREADS = TX * TY;
+// Marching kernel of the FP32 step (itlbm_march.cu): work items are 32-column strips of MARCH_SEG rows.
+constexpr int MARCH_W = 32;
+constexpr int MARCH_SEG = 64;
 
 // D3Q19 velocity set in the order of def_lattice_d3q19 (SimBoltz_Functions/LBM_functions.cpp:366-497)
 __host__ __device__ constexpr int cx(int i) {
@@ -54,6 +58,7 @@ __host__ __device__ __forceinline__ void sfor(F &&f) {
 
 // Per-case descriptor read by the step and diagnostic kernels (device memory).
 struct CaseDev {
+    CUtensorMap tmap;      // FP32 marching kernel: {nx, ny, 38, 2} view of both buffers (64-B aligned)
     void *buf[2];          // the two state buffers, each 2 x 19 arrays of `stride` elements
     double *aux;           // 4 arrays of pitch*ny doubles: Fx, Fy, Fz, |grad rho^N| (may be null)
     long long stride;      // elements per population array (pitch * ny)
@@ -65,6 +70,8 @@ struct CaseDev {
     int parity0;           // buffer index holding the state at sub-step k = 0
     int chunk_len;         // sub-steps to run in this launch sequence (INT_MAX for single cases)
     int aux_at_end;        // keep aux at sub-step chunk_len - 1
+    int march;             // FP32: 1 = marching kernel (work items = strips x segments), 0 = tiles
+    int m_strips, m_items; // marching kernel: strips per segment row, work items
     double A;              // amplitude (class P)
     double sigma;          // tension (class F)
     double beta;           // recolouring factor
@@ -93,8 +100,22 @@ void seam_perturb(int n, double A, double B0, double B1, double B2, const double
 void seam_source(int n, const double *F, const double *u, double factor, double *S);
 void seam_colisao(int n, const CaseDev &c, bool force, double *fR, double *fB, const double *gm,
                   const double *F);
+cudaError_t launch_march_f32(const CaseDev *cases_dev, const TileRef *items, int nitems,
+                             const int *nitems_dev, int grid, int k, int aux_k, cudaStream_t s);
+cudaError_t march_prepare();
+int march_error_take();
+cudaError_t encode_state_map(CaseDev &h, void *mem, size_t per_buf);
+size_t march_smem_bytes();
+// Layout of a case's state and its work items (tiles or marching items), and the binding of its
+// state block: pointers and, for the marching kernel, the tensor map.
+void case_layout(CaseDev &h, int nx, int ny, int prec, bool march);
+int case_items(const CaseDev &h);
+cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf);
+// The FP32 kernel the library uses: the marching kernel unless ITLBM_STEP_KERNEL=tile.
+bool march_default();
+// `march` selects the FP32 kernel; FP64 always runs the tile kernel.
 cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                        const int *ntiles_dev, int grid, int k, int aux_k, int prec,
+                        const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
                         cudaStream_t s);
 cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
                         cudaStream_t s);

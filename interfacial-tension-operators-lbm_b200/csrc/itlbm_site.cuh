@@ -231,26 +231,39 @@ __device__ __forceinline__ void colisao_site_f64(double (&fR)[NV], double (&fB)[
 // ---------------------------------------------------------------------------------------------
 // FP32 shifted form: e_i = f_i - w_i rho0, d_i = f_R,i - f_B,i
 // ---------------------------------------------------------------------------------------------
+// The FP32 form is evaluated by opposite-direction pairs: c_{2m} = -c_{2m-1} (m = 1..9), so the
+// pair shares c.u, the symmetric part of f_eq, c.F, (c.g)^2 and the recolouring term; the rest
+// population comes out as a complement.  (The FP64 form keeps the reference's per-direction order.)
+template <int i, class T>
+__device__ __forceinline__ T cdotp(T a, T b, T c3) {  // c_i . (a, b, c3), non-zero terms only
+    T s = T(0);
+    if constexpr (cx(i) == 1) s = a;
+    if constexpr (cx(i) == -1) s = -a;
+    if constexpr (cy(i) == 1) s = (cx(i) == 0) ? b : s + b;
+    if constexpr (cy(i) == -1) s = (cx(i) == 0) ? -b : s - b;
+    if constexpr (cz(i) == 1) s = (cx(i) == 0 && cy(i) == 0) ? c3 : s + c3;
+    if constexpr (cz(i) == -1) s = (cx(i) == 0 && cy(i) == 0) ? -c3 : s - c3;
+    return s;
+}
+
 // Recolouring split of the FP32 form: d_i = rho^N f_i - fat2 w_i cos(phi_i) with
-// fat2 = 2 beta c_R c_B rho = beta (1 - rho^N^2) rho / 2 (c_R - c_B = rho^N); d_0 is the complement
-// D - sum_{i>=1} d_i, formed by the step kernel with FP64 sums.
+// fat2 = 2 beta c_R c_B rho = beta (1 - rho^N^2) rho / 2 (c_R - c_B = rho^N) and
+// cos(phi_i) = (c_i . g) / (|c_i| |g|); k1 and k2 fold fat2 w_i / (|c_i| |g|) of the two speeds.
+// d_0 is the complement D - sum_{i>=1} d_i, formed by the step kernel with FP64 sums.
 struct Recolour32 {
-    float phi, fat2, gx, gy, gz, inv_mod;
+    float phi, k1, k2, gx, gy, gz;
     bool skip;
 };
 
+// d_i and d_{i+1} of the pair (i, i + 1), i odd, from the post-collision e_i, e_{i+1}.
 template <int i>
-__device__ __forceinline__ float split32(const Recolour32 &r, float ei, float rho0) {
+__device__ __forceinline__ void split32_pair(const Recolour32 &r, float ei, float ej, float rho0, float &di,
+                                             float &dj) {
     constexpr float w = wgt<float>(i);
-    const float f = w * rho0 + ei;
-    if constexpr (i == 0) {
-        return r.phi * f;
-    } else {
-        constexpr float rs2 = 0.70710678118654752f;
-        const float cg = (float)cx(i) * r.gx + (float)cy(i) * r.gy + (float)cz(i) * r.gz;
-        const float cosp = cg * r.inv_mod * (cc(i) == 2 ? rs2 : 1.0f);
-        return r.phi * f - r.fat2 * w * cosp;
-    }
+    const float wr = w * rho0;
+    const float K = cdotp<i>(r.gx, r.gy, r.gz) * (cc(i) == 1 ? r.k1 : r.k2);
+    di = fmaf(r.phi, wr + ei, -K);
+    dj = fmaf(r.phi, wr + ej, K);
 }
 
 // e_i = f_i - w_i rho0 in, post-collision e_i out; drho = sum e_i, D = sum d_i = rho_R - rho_B.
@@ -271,81 +284,142 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
         az = Fz * inv_rho;
     }
     float jx = 0.f, jy = 0.f, jz = 0.f;
-    sfor<0, NV>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        if constexpr (cx(i) == 1) jx += e[i];
-        if constexpr (cx(i) == -1) jx -= e[i];
-        if constexpr (cy(i) == 1) jy += e[i];
-        if constexpr (cy(i) == -1) jy -= e[i];
-        if constexpr (cz(i) == 1) jz += e[i];
-        if constexpr (cz(i) == -1) jz -= e[i];
+    sfor<0, 9>([&](auto M) {
+        constexpr int i = 2 * decltype(M)::value + 1;
+        const float p = e[i] - e[i + 1];
+        if constexpr (cx(i) == 1) jx += p;
+        if constexpr (cx(i) == -1) jx -= p;
+        if constexpr (cy(i) == 1) jy += p;
+        if constexpr (cy(i) == -1) jy -= p;
+        if constexpr (cz(i) == 1) jz += p;
+        if constexpr (cz(i) == -1) jz -= p;
     });
-    const float vx = jx * inv_rho + 0.5f * ax, vy = jy * inv_rho + 0.5f * ay;
-    const float vz = jz * inv_rho + 0.5f * az;
+    const float vx = fmaf(jx, inv_rho, 0.5f * ax), vy = fmaf(jy, inv_rho, 0.5f * ay);
+    const float vz = fmaf(jz, inv_rho, 0.5f * az);
     const float usq15 = 1.5f * (vx * vx + vy * vy + vz * vz);
     const float inv_tau = (float)c.inv_tau;
+    const float rho3 = 3.0f * rho;
     const float Frx = ax * rho, Fry = ay * rho, Frz = az * rho;
     const float vF = Frx * vx + Fry * vy + Frz * vz;
     const float fac3 = 3.0f * (float)c.src_factor;
-    sfor<0, NV>([&](auto I) {
-        constexpr int i = decltype(I)::value;
+    // BGK (+ Guo source) of the moving populations:
+    //   f_eq - w rho0 = w (drho + rho (4.5 cu^2 - 1.5 u^2) +- 3 rho cu)
+    //   S = 3 (1 - 1/2tau) w (3 (c.F)(c.u) - u.F +- c.F)
+    sfor<0, 9>([&](auto M) {
+        constexpr int i = 2 * decltype(M)::value + 1;
         constexpr float w = wgt<float>(i);
-        const float cu = (float)cx(i) * vx + (float)cy(i) * vy + (float)cz(i) * vz;
-        // f_eq - w rho0 = w (drho + rho (3 cu + 4.5 cu^2 - 1.5 u^2))
-        const float dfeq = w * (drho + rho * (cu * (3.0f + 4.5f * cu) - usq15));
-        float en = e[i] + (dfeq - e[i]) * inv_tau;
+        const float cu = cdotp<i>(vx, vy, vz);
+        const float sym = w * fmaf(rho, fmaf(4.5f * cu, cu, -usq15), drho);
+        const float asym = (w * rho3) * cu;
+        float ei = fmaf((sym + asym) - e[i], inv_tau, e[i]);
+        float ej = fmaf((sym - asym) - e[i + 1], inv_tau, e[i + 1]);
         if constexpr (FORCE) {
-            const float cF = (float)cx(i) * Frx + (float)cy(i) * Fry + (float)cz(i) * Frz;
-            en += (fac3 * w) * (cF + 3.0f * cF * cu - vF);
+            const float cF = cdotp<i>(Frx, Fry, Frz);
+            const float P = fmaf(3.0f * cF, cu, -vF);
+            ei = fmaf(fac3 * w, P + cF, ei);
+            ej = fmaf(fac3 * w, P - cF, ej);
         }
-        e[i] = en;
+        e[i] = ei;
+        e[i + 1] = ej;
     });
     const float mod2 = gmx * gmx + gmy * gmy + gmz * gmz;
     const float mod = sqrtf(mod2);
     if constexpr (!FORCE) {
+        // class P: f_i += A |g| (w_i (c_i.g)^2 / |g|^2 - B_i), the same for both of a pair
         const float A = (float)c.A;
         if (!(mod2 <= 1.0e-30f || A == 0.0f)) {
             const float inv2 = 1.0f / mod2;
             const float amod = A * mod;
-            sfor<0, NV>([&](auto I) {
-                constexpr int i = decltype(I)::value;
+            const float B1 = (float)c.B1, B2 = (float)c.B2;
+            sfor<0, 9>([&](auto M) {
+                constexpr int i = 2 * decltype(M)::value + 1;
                 constexpr float w = wgt<float>(i);
-                const float cg = (float)cx(i) * gmx + (float)cy(i) * gmy + (float)cz(i) * gmz;
-                const float B = (float)(cc(i) == 0 ? c.B0 : (cc(i) == 1 ? c.B1 : c.B2));
-                e[i] += amod * (w * cg * cg * inv2 - B);
+                const float cg = cdotp<i>(gmx, gmy, gmz);
+                const float om = amod * fmaf(w * cg, cg * inv2, -(cc(i) == 1 ? B1 : B2));
+                e[i] += om;
+                e[i + 1] += om;
             });
         }
     }
-    // Every site update conserves the mass (sum e_i = drho) and the colour difference (sum d_i = D)
-    // exactly; in float arithmetic the weights do not sum to 1 (1 + 1.5e-8), which would bias both
-    // sums every step.  The rest populations e_0 and d_0 are therefore formed as the complements.
+    // Every site update conserves the mass (sum e_i = drho) exactly; in float arithmetic the weights
+    // do not sum to 1 (1 + 1.5e-8), which would bias the sum every step.  The rest population e_0 is
+    // therefore the complement.
     {
-        float s = 0.f;
-        sfor<1, NV>([&](auto I) { s += e[decltype(I)::value]; });
-        e[0] = drho - s;
+        float s0 = (e[1] + e[2]) + (e[3] + e[4]), s1 = (e[5] + e[6]) + (e[7] + e[8]);
+        float s2 = (e[9] + e[10]) + (e[11] + e[12]), s3 = (e[13] + e[14]) + (e[15] + e[16]);
+        e[0] = drho - (((s0 + s1) + (s2 + s3)) + (e[17] + e[18]));
     }
+    const float fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
+    const float inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
     rc.phi = phi;
-    rc.fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
-    rc.inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
+    rc.k1 = fat2 * wgt<float>(1) * inv_mod;
+    rc.k2 = fat2 * wgt<float>(7) * 0.70710678118654752f * inv_mod;
     rc.gx = gmx;
     rc.gy = gmy;
     rc.gz = gmz;
+}
+
+// FP32 stencils by pairs (the FP64 path uses the per-direction forms below, in the reference's
+// order).  Mediator momentum sum_i c_i w_i 3 phi(x - c_i); the isotropic gradient
+// 3 sum_i w_i c_i phi(x + c_i) is its exact negative.
+template <class P>
+__device__ __forceinline__ void mediator_grad_f32(P phi, float &gx, float &gy, float &gz) {
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    sfor<0, 9>([&](auto M) {
+        constexpr int i = 2 * decltype(M)::value + 1;
+        constexpr float w3 = 3.0f * wgt<float>(i);
+        const float dphi = w3 * (phi(-cx(i), -cy(i)) - phi(cx(i), cy(i)));
+        if constexpr (cx(i) == 1) ax += dphi;
+        if constexpr (cx(i) == -1) ax -= dphi;
+        if constexpr (cy(i) == 1) ay += dphi;
+        if constexpr (cy(i) == -1) ay -= dphi;
+        if constexpr (cz(i) == 1) az += dphi;
+        if constexpr (cz(i) == -1) az -= dphi;
+    });
+    gx = ax;
+    gy = ay;
+    gz = az;
+}
+template <class P>
+__device__ __forceinline__ void iso_grad_f32(P phi, float &gx, float &gy, float &gz) {
+    mediator_grad_f32(phi, gx, gy, gz);
+    gx = -gx;
+    gy = -gy;
+    gz = -gz;
+}
+// F3 chemical potential mu = 4 b phi (phi^2 - 1) - k lap phi, lap = 6 sum_i w_i (phi(x + c_i) - phi)
+template <class P>
+__device__ __forceinline__ float chem_pot_f32(P phi, float kf, float bf) {
+    const float ph = phi(0, 0);
+    float l1 = 0.f, l2 = 0.f;
+    sfor<0, 9>([&](auto M) {
+        constexpr int i = 2 * decltype(M)::value + 1;
+        const float s = phi(cx(i), cy(i)) + phi(-cx(i), -cy(i));
+        if constexpr (cc(i) == 1) l1 += s;
+        else l2 += s;
+    });
+    // sum_i w_i (phi_i - ph) = (l1 - 6 ph) / 18 + (l2 - 12 ph) / 36
+    const float lap = 6.0f * (fmaf(-6.0f, ph, l1) * (1.0f / 18.0f) + fmaf(-12.0f, ph, l2) * (1.0f / 36.0f));
+    return 4.0f * bf * ph * (ph * ph - 1.0f) - kf * lap;
 }
 
 // ---------------------------------------------------------------------------------------------
 // Stencils on a staged phase tile, generic in the real type
 // ---------------------------------------------------------------------------------------------
 
-// Mediator momentum at tile position (px, py): sum_i c_i * (w_i * (phi(x - c_i) * 3)), the
-// momentum() (LBM_functions.cpp:1057-1087) of the mediators after emite_mediadores + propag_site_med
+// The stencils below read the staged phase field through an accessor P(dx, dy) = rho^N at
+// (x + dx, y + dy), so that the tile kernel (a plain 2-D array) and the marching kernel (a ring of
+// rows) evaluate them with the same arithmetic in the same order.
+
+// Mediator momentum at the node: sum_i c_i * (w_i * (phi(x - c_i) * 3)), the momentum()
+// (LBM_functions.cpp:1057-1087) of the mediators after emite_mediadores + propag_site_med
 // (LBM_functions.cpp:1287-1337), accumulated in index order.
-template <class T, int W_>
-__device__ __forceinline__ void mediator_grad(const T (*phi)[W_], int px, int py, T &gx, T &gy,
-                                              T &gz) {
+template <class T, class P>
+__device__ __forceinline__ void mediator_grad_at(P phi, T &gx, T &gy, T &gz) {
     T ax = T(0), ay = T(0), az = T(0);
     sfor<0, NV>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        const T M = wgt<T>(i) * (phi[py - cy(i)][px - cx(i)] * T(3));
+        const T M = wgt<T>(i) * (phi(-cx(i), -cy(i)) * T(3));
         if constexpr (cx(i) == 1) ax = ax + M;
         if constexpr (cx(i) == -1) ax = ax - M;
         if constexpr (cy(i) == 1) ay = ay + M;
@@ -359,12 +433,12 @@ __device__ __forceinline__ void mediator_grad(const T (*phi)[W_], int px, int py
 }
 
 // Isotropic gradient 3 sum_{i>=1} w_i c_i phi(x + c_i) (Operadores_tensao.cpp:219-235).
-template <class T, int W_>
-__device__ __forceinline__ void iso_grad(const T (*phi)[W_], int px, int py, T &gx, T &gy, T &gz) {
+template <class T, class P>
+__device__ __forceinline__ void iso_grad_at(P phi, T &gx, T &gy, T &gz) {
     T ax = T(0), ay = T(0), az = T(0);
     sfor<1, NV>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        const T ph = wgt<T>(i) * phi[py + cy(i)][px + cx(i)];
+        const T ph = wgt<T>(i) * phi(cx(i), cy(i));
         if constexpr (cx(i) == 1) ax += ph;
         if constexpr (cx(i) == -1) ax -= ph;
         if constexpr (cy(i) == 1) ay += ph;
@@ -378,16 +452,31 @@ __device__ __forceinline__ void iso_grad(const T (*phi)[W_], int px, int py, T &
 }
 
 // F3 chemical potential mu = 4 b phi (phi^2 - 1) - k lap phi (Operadores_tensao.cpp:273-287).
-template <class T, int W_>
-__device__ __forceinline__ T chem_pot(const T (*phi)[W_], int px, int py, T kf, T bf) {
-    const T ph = phi[py][px];
+template <class T, class P>
+__device__ __forceinline__ T chem_pot_at(P phi, T kf, T bf) {
+    const T ph = phi(0, 0);
     T lap = T(0);
     sfor<1, NV>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        lap += wgt<T>(i) * (phi[py + cy(i)][px + cx(i)] - ph);
+        lap += wgt<T>(i) * (phi(cx(i), cy(i)) - ph);
     });
     lap *= T(6);
     return T(4) * bf * ph * (ph * ph - T(1)) - kf * lap;
+}
+
+// the same on a staged 2-D tile at position (px, py)
+template <class T, int W_>
+__device__ __forceinline__ void mediator_grad(const T (*phi)[W_], int px, int py, T &gx, T &gy,
+                                              T &gz) {
+    mediator_grad_at<T>([&](int dx, int dy) { return phi[py + dy][px + dx]; }, gx, gy, gz);
+}
+template <class T, int W_>
+__device__ __forceinline__ void iso_grad(const T (*phi)[W_], int px, int py, T &gx, T &gy, T &gz) {
+    iso_grad_at<T>([&](int dx, int dy) { return phi[py + dy][px + dx]; }, gx, gy, gz);
+}
+template <class T, int W_>
+__device__ __forceinline__ T chem_pot(const T (*phi)[W_], int px, int py, T kf, T bf) {
+    return chem_pot_at<T>([&](int dx, int dy) { return phi[py + dy][px + dx]; }, kf, bf);
 }
 
 // F1 unit normal (Operadores_tensao.cpp:251-258) and F2 stress (:259-272) from the gradient.
@@ -412,13 +501,14 @@ __device__ __forceinline__ void aux_stress(T gx, T gy, T gz, T sigma, T *a) {
     a[5] = -h * gy * gz * inv;
 }
 
-// F1: kappa = -div_iso(n) (Operadores_tensao.cpp:187-200, :298-305).  aux has AS components.
-template <class T, int AS, int W_>
-__device__ __forceinline__ T curvature(const T (*aux)[W_][AS], int qx, int qy) {
+// F1: kappa = -div_iso(n) (Operadores_tensao.cpp:187-200, :298-305).  A(dx, dy) points at the
+// auxiliary components of node (x + dx, y + dy), the normal in components 0..2.
+template <class T, class A>
+__device__ __forceinline__ T curvature_at(A aux) {
     T d = T(0);
     sfor<1, NV>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        const T *v = aux[qy + cy(i)][qx + cx(i)];
+        const T *v = aux(cx(i), cy(i));
         T s = T(0);
         bool first = true;
         auto add = [&](int ci, T val) {
@@ -436,13 +526,12 @@ __device__ __forceinline__ T curvature(const T (*aux)[W_][AS], int qx, int qy) {
 }
 
 // F2: F_a = 3 sum_i w_i T_ab(x + c_i) c_ib (Operadores_tensao.cpp:306-324).
-template <class T, int AS, int W_>
-__device__ __forceinline__ void stress_div(const T (*aux)[W_][AS], int qx, int qy, T &Fx, T &Fy,
-                                           T &Fz) {
+template <class T, class A>
+__device__ __forceinline__ void stress_div_at(A aux, T &Fx, T &Fy, T &Fz) {
     T ax = T(0), ay = T(0), az = T(0);
     sfor<1, NV>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        const T *t = aux[qy + cy(i)][qx + cx(i)];
+        const T *t = aux(cx(i), cy(i));
         auto dotc = [&](T a, T b, T c3) {
             T s = T(0);
             bool first = true;
@@ -465,6 +554,16 @@ __device__ __forceinline__ void stress_div(const T (*aux)[W_][AS], int qx, int q
     Fx = T(3) * ax;
     Fy = T(3) * ay;
     Fz = T(3) * az;
+}
+
+template <class T, int AS, int W_>
+__device__ __forceinline__ T curvature(const T (*aux)[W_][AS], int qx, int qy) {
+    return curvature_at<T>([&](int dx, int dy) { return aux[qy + dy][qx + dx]; });
+}
+template <class T, int AS, int W_>
+__device__ __forceinline__ void stress_div(const T (*aux)[W_][AS], int qx, int qy, T &Fx, T &Fy,
+                                           T &Fz) {
+    stress_div_at<T>([&](int dx, int dy) { return aux[qy + dy][qx + dx]; }, Fx, Fy, Fz);
 }
 
 }  // namespace itlbm

@@ -175,7 +175,9 @@ cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case
     double *dprof = nullptr;
     cudaError_t e = cudaMalloc(&dprof, sizeof(double) * prof.size());
     if (e != cudaSuccess) return e;
-    e = cudaMemcpy(dprof, prof.data(), sizeof(double) * prof.size(), cudaMemcpyHostToDevice);
+    // on the launch stream: a pageable copy may return before its data has reached the device, and
+    // a non-blocking stream is not ordered after the legacy stream
+    e = cudaMemcpyAsync(dprof, prof.data(), sizeof(double) * prof.size(), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         k_init<<<grid_for(n, 256), 256, 0, s>>>(c_dev, d.geometry, dprof, d.v0, d.rho_R, d.rho_B,
                                                 d.p, d.q);

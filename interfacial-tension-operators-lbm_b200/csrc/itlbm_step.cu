@@ -134,8 +134,16 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #pragma unroll
             for (int i = 0; i < NV; i++) v[i] = __ldg(p + (long long)i * stride);
             S acc = S(0);
+            if (std::is_same<S, float>::value && colour == 1) {
+                // FP32: the colour difference summed in FP64, as for the tile's own nodes
+                double a = 0.0;
 #pragma unroll
-            for (int i = 0; i < NV; i++) acc = acc + v[i];
+                for (int i = 0; i < NV; i++) a += (double)v[i];
+                acc = (S)a;
+            } else {
+#pragma unroll
+                for (int i = 0; i < NV; i++) acc = acc + v[i];
+            }
             sm.rsum[colour][r] = acc;
         }
     }
@@ -156,7 +164,10 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             const int gx = x0 - 1 + qx, gy = y0 - 1 + qy;
             if (gx < xe + 1 && gy < ye + 1) {
                 S g0, g1, g2;
-                iso_grad(sm.phi, qx + 1, qy + 1, g0, g1, g2);
+                if constexpr (std::is_same<S, float>::value)
+                    iso_grad_f32([&](int dx, int dy) { return sm.phi[qy + 1 + dy][qx + 1 + dx]; }, g0, g1, g2);
+                else
+                    iso_grad(sm.phi, qx + 1, qy + 1, g0, g1, g2);
                 sm.g[qy][qx][0] = g0;
                 sm.g[qy][qx][1] = g1;
                 sm.g[qy][qx][2] = g2;
@@ -171,7 +182,9 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     if (valid) {
         const int px = lx + HMAX, py = ly + HMAX;
         S gmx, gmy, gmz;
-        mediator_grad(sm.phi, px, py, gmx, gmy, gmz);
+        auto phi_at = [&](int dx, int dy) { return sm.phi[py + dy][px + dx]; };
+        if constexpr (std::is_same<S, float>::value) mediator_grad_f32(phi_at, gmx, gmy, gmz);
+        else mediator_grad(sm.phi, px, py, gmx, gmy, gmz);
         S Fx = S(0), Fy = S(0), Fz = S(0);
         const bool force = tipo >= ITLBM_OP_F1;
         if (tipo == ITLBM_OP_F1) {
@@ -184,9 +197,16 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         } else if (tipo == ITLBM_OP_F2) {
             stress_div<S, 6>(sm.aux, lx + 1, ly + 1, Fx, Fy, Fz);
         } else if (tipo == ITLBM_OP_F3) {
-            S g0, g1, g2;
-            iso_grad(sm.phi, px, py, g0, g1, g2);
-            const S mu = chem_pot(sm.phi, px, py, (S)c.kf, (S)c.bf);
+            S g0, g1, g2, mu;
+            if constexpr (std::is_same<S, float>::value) {
+                g0 = -gmx;  // the isotropic gradient is the exact negative of the mediator momentum
+                g1 = -gmy;
+                g2 = -gmz;
+                mu = chem_pot_f32(phi_at, (float)c.kf, (float)c.bf);
+            } else {
+                iso_grad(sm.phi, px, py, g0, g1, g2);
+                mu = chem_pot(sm.phi, px, py, (S)c.kf, (S)c.bf);
+            }
             Fx = mu * g0;
             Fy = mu * g1;
             Fz = mu * g2;
@@ -226,13 +246,17 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                 // steps); in FP64 the only rounding left is that of d_0 itself.
                 const float rho0 = (float)c.rho0;
                 double dsum = 0.0;
-                sfor<1, NV>([&](auto I) {
-                    constexpr int i = decltype(I)::value;
-                    const long long o = dst_off(i);
-                    const float d = split32<i>(rc, f[i], rho0);
-                    dsum += (double)d;
-                    dst[(long long)i * stride + o] = f[i];
-                    dst[(long long)(NV + i) * stride + o] = d;
+                sfor<0, 9>([&](auto M) {
+                    constexpr int i = 2 * decltype(M)::value + 1;
+                    float di, dj;
+                    split32_pair<i>(rc, f[i], f[i + 1], rho0, di, dj);
+                    dsum += (double)di;
+                    dsum += (double)dj;
+                    const long long oi = dst_off(i), oj = dst_off(i + 1);
+                    dst[(long long)i * stride + oi] = f[i];
+                    dst[(long long)(NV + i) * stride + oi] = di;
+                    dst[(long long)(i + 1) * stride + oj] = f[i + 1];
+                    dst[(long long)(NV + i + 1) * stride + oj] = dj;
                 });
                 const long long o0 = dst_off(0);
                 dst[o0] = f[0];

@@ -116,6 +116,69 @@ def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600):
     return upd // steps, ms, (sampler.summary() if sampler else None), st1.active
 
 
+def served_stream(seed=20261203, n=160):
+    """The served-stream configuration, scaled to a bench run: Poisson arrivals of cases with side
+    log-uniform in 64-1024, 500-5000 steps (the full stream is 64-2048 and 5 000-100 000 steps),
+    10 % FP64, 80 % drops / 20 % inclined strips, operators, tau and sigma as in the batch mix."""
+    import numpy as np
+    rng = np.random.default_rng(seed + 1)
+    ops = [(1, 0.5), (3, -0.4), (3, 0.5), (3, 2.0), (11, 0.5), (12, 0.5), (13, 0.5)]
+    reqs = []
+    for _ in range(n):
+        side = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        strip = rng.uniform() < 0.2
+        tipo, chi = ops[rng.integers(len(ops))]
+        tau = float(rng.uniform(0.51, 2.0))
+        sigma = float(math.exp(rng.uniform(math.log(0.1), math.log(2.0))))
+        A = 9.0 * sigma / (4.0 * tau) if tipo < 11 else sigma
+        p, q = (int(rng.integers(1, 5)), int(rng.integers(1, 5))) if strip else (1, 0)
+        radius = float(rng.uniform(10.0, side / 4.0)) if not strip else 0.0
+        reqs.append(dict(nx=side, tipo=tipo, chi=chi, tau=tau, A=A, strip=strip, p=p, q=q, radius=radius,
+                         steps=int(rng.integers(500, 5001)), fp64=bool(rng.uniform() < 0.1)))
+    gaps = rng.exponential(1.0, n)
+    return reqs, gaps
+
+
+def served_latency(pkg, load=0.7, capacity_mlups=8000.0):
+    """Time-to-result of a stream of cases fed into one batch as they arrive (Poisson, offered load
+    `load` of `capacity_mlups`): from submission to the case's last step and diagnostic, wall clock."""
+    import numpy as np
+    reqs, gaps = served_stream()
+    work = np.mean([r["nx"] ** 2 * r["steps"] for r in reqs])
+    rate = load * capacity_mlups * 1e6 / work  # arrivals per second
+    arrive = np.cumsum(gaps / rate)
+    b = pkg.Batch(chunk=250, diag_every=500)
+    t0 = time.perf_counter()
+    nxt, lat, done = 0, [], 0
+    while done < len(reqs):
+        now = time.perf_counter() - t0
+        while nxt < len(reqs) and arrive[nxt] <= now:
+            r = reqs[nxt]
+            b.submit(batch_desc(pkg, r, pkg.PREC_F64 if r["fp64"] else pkg.PREC_F32), r["steps"], nxt)
+            nxt += 1
+        st = b.stats()
+        if st.active == 0 and st.pending == 0:
+            if nxt < len(reqs):
+                time.sleep(min(0.001, max(0.0, arrive[nxt] - now)))
+            continue
+        b.advance()
+        for e in b.poll():
+            if e.kind != pkg.EV_DIAG:
+                lat.append(e.t_event - e.t_submit)
+                done += 1
+    wall = time.perf_counter() - t0
+    st = b.stats()
+    b.close()
+    lat = np.sort(np.array(lat))
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "max_s": float(lat[-1]), "requests": len(reqs), "offered_load": load,
+            "offered_mlups": load * capacity_mlups, "achieved_mlups": st.node_updates / wall / 1e6,
+            "wall_s": wall,
+            "workload": "served stream, scaled: Poisson arrivals, side 64-1024, 500-5000 steps, 10% FP64, "
+                        "80% drops / 20% strips, 7 operators; time-to-result from submission to the last "
+                        "step's diagnostic"}
+
+
 def batch_e2e(pkg, steps, n_cases=600):
     """The batch through the C ABI, wall clock: submit every case, advance until each has run
     `steps` steps (diagnostics every 500 steps fall due on the way), poll the events."""
@@ -381,6 +444,7 @@ def main():
     ap.add_argument("--workload", default="batch600", choices=["batch600"] + sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-latency", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -399,7 +463,7 @@ def main():
         nodes, ms, clocks, ncases = batch_run(pkg, args.steps, args.warmup, world, rank == 0, local)
         mlups, ms_max = replica_mlups(nodes * args.steps, ms, world)
         achieved = 304.0 * nodes * args.steps / (ms * 1e-3) / 1e9
-        launches = 2 * args.steps  # one FP64 and one FP32 persistent launch per step (no FP64 cases here)
+        launches = args.steps  # one FP32 launch per step; the FP64 table is empty, so nothing is launched for it
         cfg = batch_config(nodes, ncases, world)
     else:
         nodes, ms, clocks = device_run(pkg, single, pkg.PREC_F32, args.steps, args.warmup, world,
@@ -425,6 +489,9 @@ def main():
         e2e = batch_e2e(pkg, 1001) if args.workload == "batch600" else e2e_run(pkg, single, pkg.PREC_F32, args.steps)
         if world > 1:
             e2e["value"] = allreduce_sum(e2e["value"], world)
+    latency = None
+    if not args.no_latency and args.workload == "batch600":
+        latency = served_latency(pkg, capacity_mlups=0.8 * mlups / world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -444,6 +511,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
             "e2e": e2e,
+            "latency": latency,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

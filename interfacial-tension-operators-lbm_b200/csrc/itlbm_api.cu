@@ -66,7 +66,7 @@ cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntil
 
 bool march_default() {
     const char *v = getenv("ITLBM_STEP_KERNEL");
-    return !(v && std::strcmp(v, "tile") == 0);
+    return v && std::strcmp(v, "march") == 0;
 }
 
 void case_layout(CaseDev &h, int nx, int ny, int prec, bool march) {

@@ -80,7 +80,7 @@ struct itlbm_batch {
     int *d_ntiles = nullptr;
     bool tables_dirty = true;
     int grid[2] = {0, 0};
-    bool march = true;  // FP32 cases run the marching kernel
+    bool march = false;  // FP32 cases run the marching kernel
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DiagScratch diag;

@@ -556,12 +556,16 @@ __device__ double fase_em(const double *__restrict__ node, long long n, int nx, 
     if (!isfinite(x) || !isfinite(y)) return 0.0;  // keeps every index below in range
     x = x - nx * floor(x / nx);
     y = y - ny * floor(y / ny);
-    const int i0 = (int)floor(x), j0 = (int)floor(y);
+    const int i0 = (int)floor(x), j0 = (int)floor(y);  // in [0, nx] x [0, ny]
     const double tx = x - i0, ty = y - j0;
     double v = 0.0;
     for (int dj = 0; dj < 2; dj++)
         for (int di = 0; di < 2; di++) {
-            const int ii = ((i0 + di) % nx + nx) % nx, jj = ((j0 + dj) % ny + ny) % ny;
+            int ii = i0 + di, jj = j0 + dj;  // periodic image, without integer division
+            if (ii >= nx) ii -= nx;
+            if (ii >= nx) ii -= nx;
+            if (jj >= ny) jj -= ny;
+            if (jj >= ny) jj -= ny;
             const long long p = ii + (long long)jj * nx;
             const double rR = node[p], rB = node[n + p];
             const double wgt2 = (di ? tx : 1 - tx) * (dj ? ty : 1 - ty);
@@ -591,21 +595,28 @@ __global__ void __launch_bounds__(ITLBM_N_ANG) k_drop_modes(const CaseDev *__res
         else b = mid;
     }
     const double r = 0.5 * (a + b);
-    __shared__ double rs[ITLBM_N_ANG];
-    rs[k] = r;
+    // each ray forms its own harmonic products; one thread then sums them in ray order, as the
+    // reference loop does
+    __shared__ double rs[7][ITLBM_N_ANG];
+    rs[0][k] = r;
+    rs[1][k] = r * cos(2 * th);
+    rs[2][k] = r * sin(2 * th);
+    rs[3][k] = r * cos(4 * th);
+    rs[4][k] = r * sin(4 * th);
+    rs[5][k] = r * cos(8 * th);
+    rs[6][k] = r * sin(8 * th);
     __syncthreads();
     if (k == 0) {
-        // sums in ray order, as the reference loop
         double c2 = 0, s2 = 0, c4 = 0, s4 = 0, c8 = 0, s8 = 0, soma = 0, rmin = 1e30, rmax = 0;
         for (int j = 0; j < N_ANG; j++) {
-            const double t = 2.0 * 3.14159265358979323846 * j / N_ANG, rr = rs[j];
+            const double rr = rs[0][j];
             soma += rr;
-            c2 += rr * cos(2 * t);
-            s2 += rr * sin(2 * t);
-            c4 += rr * cos(4 * t);
-            s4 += rr * sin(4 * t);
-            c8 += rr * cos(8 * t);
-            s8 += rr * sin(8 * t);
+            c2 += rs[1][j];
+            s2 += rs[2][j];
+            c4 += rs[3][j];
+            s4 += rs[4][j];
+            c8 += rs[5][j];
+            s8 += rs[6][j];
             rmin = fmin(rmin, rr);
             rmax = fmax(rmax, rr);
         }

@@ -17,7 +17,10 @@ constexpr int NV = 19;
 // Tile of the fused step: TX x TY interior nodes, one per thread; the phase field is staged with a
 // halo of up to HMAX nodes (1 for P1/P3/F3, 2 for F1/F2).
 constexpr int TX = 32;
-constexpr int TY = 8;
+#ifndef ITLBM_TILE_ROWS
+#define ITLBM_TILE_ROWS 8
+#endif
+constexpr int TY = ITLBM_TILE_ROWS;
 constexpr int HMAX = 2;
 constexpr int PX = TX + 2 * HMAX;  // staged phase tile width
 constexpr int PY = TY + 2 * HMAX;  // staged phase tile height
@@ -111,7 +114,7 @@ size_t march_smem_bytes();
 void case_layout(CaseDev &h, int nx, int ny, int prec, bool march);
 int case_items(const CaseDev &h);
 cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf);
-// The FP32 kernel the library uses: the marching kernel unless ITLBM_STEP_KERNEL=tile.
+// The FP32 kernel the library uses: the tile kernel, or the marching kernel with ITLBM_STEP_KERNEL=march.
 bool march_default();
 // `march` selects the FP32 kernel; FP64 always runs the tile kernel.
 cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,

@@ -41,6 +41,7 @@ struct MarchSmem {
     alignas(128) float d[2][MR][ROWF];     // d-planes of two slabs
     float phi[PR][BW];                     // rho^N, column index x - x0 + 4
     double D[NR][MW];                      // sum d_i of the interior nodes (FP64)
+    float Df[NR][MW];                      // the same in FP32, as rho^N uses it
     float drho[NR][MW];                    // sum e_i of the interior nodes
     float aux[NR][AW][6];                  // F1: normal 0..2, gradient 3..5; F2: stress 0..5
     alignas(8) unsigned long long bar[3];  // one per e-slot: both copies of a slab complete on it
@@ -159,26 +160,33 @@ __device__ __forceinline__ void phi_pass(const CaseDev &c, const Item &it, int s
         const int r = r0 + q / cols;
         const int col = it.x0 - H + q % cols;
         const int bx = col - it.x0 + 4;  // staged column
-        float sa = 0.f;
+        const int lx = col - it.x0;
+        const bool own = (r >= it.y0 && r < it.y1 && lx >= 0 && lx < MW);
+        float sa = 0.f, sb = 0.f;
         double sbd = 0.0;
+        float d[NV];
         if (col >= 0 && col < c.nx) {
             const float *pe = &sm.e[es][r - base][bx];
             const float *pd = &sm.d[ds][r - base][bx];
 #pragma unroll
             for (int i = 0; i < NV; i++) sa = sa + pe[i * BW];
 #pragma unroll
-            for (int i = 0; i < NV; i++) sbd += (double)pd[i * BW];
+            for (int i = 0; i < NV; i++) d[i] = pd[i * BW];
         } else {  // periodic wrap in x: not in the copy
             const long long off = (long long)wrapm(r, c.ny) * c.pitch + wrapm(col, c.nx);
 #pragma unroll
             for (int i = 0; i < NV; i++) sa = sa + __ldg(src + (long long)i * c.stride + off);
 #pragma unroll
-            for (int i = 0; i < NV; i++) sbd += (double)__ldg(src + (long long)(NV + i) * c.stride + off);
+            for (int i = 0; i < NV; i++) d[i] = __ldg(src + (long long)(NV + i) * c.stride + off);
         }
-        sm.phi[(r - it.y0 + PR) & (PR - 1)][bx] = (float)sbd / (rho0 + sa);
-        const int lx = col - it.x0;
-        if (r >= it.y0 && r < it.y1 && lx >= 0 && lx < MW) {
+#pragma unroll
+        for (int i = 0; i < NV; i++) sb = sb + d[i];
+        sm.phi[(r - it.y0 + PR) & (PR - 1)][bx] = sb / (rho0 + sa);
+        if (own) {
+#pragma unroll
+            for (int i = 0; i < NV; i++) sbd += (double)d[i];
             sm.D[(r - it.y0 + NR) & (NR - 1)][lx] = sbd;
+            sm.Df[(r - it.y0 + NR) & (NR - 1)][lx] = sb;
             sm.drho[(r - it.y0 + NR) & (NR - 1)][lx] = sa;
         }
     }
@@ -222,7 +230,7 @@ __device__ __forceinline__ void collide_row(const CaseDev &c, const Item &it, in
     const int rr = (r - it.y0 + NR) & (NR - 1);
     const float sa = sm.drho[rr][lane];
     const double sbd = sm.D[rr][lane];
-    const float sb = (float)sbd;
+    const float sb = sm.Df[rr][lane];
     const int pr = r - it.y0 + PR, bx = lane + 4;
     auto phi = [&](int dx, int dy) { return sm.phi[(pr + dy) & (PR - 1)][bx + dx]; };
     float gmx, gmy, gmz;

@@ -103,14 +103,13 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         for (int i = 0; i < NV; i++) b[i] = __ldg(src + (long long)(NV + i) * stride + off);
 #pragma unroll
         for (int i = 0; i < NV; i++) sa = sa + a[i];
+#pragma unroll
+        for (int i = 0; i < NV; i++) sb = sb + b[i];
         if constexpr (std::is_same<S, float>::value) {
-            // FP32: the colour difference D = sum d_i in FP64 (see the split below)
+            // FP32: rho^N from the FP32 sums (as for the halo nodes); the colour difference is also
+            // summed in FP64 for the rest population's complement (see the split below)
 #pragma unroll
             for (int i = 0; i < NV; i++) sbd += (double)b[i];
-            sb = (float)sbd;
-        } else {
-#pragma unroll
-            for (int i = 0; i < NV; i++) sb = sb + b[i];
         }
         if constexpr (std::is_same<S, double>::value) {
 #pragma unroll
@@ -134,16 +133,8 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #pragma unroll
             for (int i = 0; i < NV; i++) v[i] = __ldg(p + (long long)i * stride);
             S acc = S(0);
-            if (std::is_same<S, float>::value && colour == 1) {
-                // FP32: the colour difference summed in FP64, as for the tile's own nodes
-                double a = 0.0;
 #pragma unroll
-                for (int i = 0; i < NV; i++) a += (double)v[i];
-                acc = (S)a;
-            } else {
-#pragma unroll
-                for (int i = 0; i < NV; i++) acc = acc + v[i];
-            }
+            for (int i = 0; i < NV; i++) acc = acc + v[i];
             sm.rsum[colour][r] = acc;
         }
     }
@@ -287,10 +278,16 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 
 // Resident CTAs per SM the register allocation is sized for: 2 x 256 threads for FP64, 4 x 256
 // threads for FP32 (the kernel is latency-bound at lower occupancy; see the ncu summaries).
+#ifndef ITLBM_F64_BLOCKS
+#define ITLBM_F64_BLOCKS 2
+#endif
+#ifndef ITLBM_F32_BLOCKS
+#define ITLBM_F32_BLOCKS 4
+#endif
 #ifdef ITLBM_STEP_F64
-#define ITLBM_STEP_MIN_BLOCKS 2
+#define ITLBM_STEP_MIN_BLOCKS (ITLBM_F64_BLOCKS * 256 / STEP_THREADS)
 #else
-#define ITLBM_STEP_MIN_BLOCKS 4
+#define ITLBM_STEP_MIN_BLOCKS (ITLBM_F32_BLOCKS * 256 / STEP_THREADS)
 #endif
 
 template <class S>

@@ -7,8 +7,9 @@ Default workload ("batch600"): a batched stream of 600 cases drawn from
 seed 20261203: square boxes with side log-uniform in 64-512, 80 % static drops (R uniform in 10 to
 side/4) and 20 % straight interfaces inclined at atan(q/p), p, q in 1..4; operator uniform over the
 seven; tau uniform in 0.51-2; sigma log-uniform in 0.1-2 (A = 9 sigma / 4 tau for class P); FP32
-shifted storage -- all advanced together by the batch engine (one CUDA graph of persistent step
-launches over the device work table).  A "step" is one lattice-Boltzmann time step of every case.
+shifted storage -- all advanced together by the batch engine (one CUDA graph of step launches over
+the device work table, one CTA per tile).  A "step" is one lattice-Boltzmann time step of every
+case.
 Beside it, one 4096 x 4096 x 1 static drop (R = 400, P3 chi = 0.5, A = 0.225, tau = 1), the
 single-case roofline configuration, in FP32 and in the plain FP64 path (bit-identical to the
 reference).
@@ -22,6 +23,10 @@ e2e     the same metric through the C ABI as a user runs the batch: itlbm_batch_
         clock from the first submit to the last step.
 roofline algorithmic bytes per update: 38 populations read + 38 written (304 B in FP32, 608 B in
         FP64) x nodes / mean kernel duration, against the measured copy bandwidth.
+fp64_one_at_a_time_mix  the plain FP64 path on the same mixed sweep, one case at a time (every
+        10th case of the mix, 40 steps each): the denominator of the batched-vs-plain ratio.
+latency the served stream (Poisson arrivals, scaled to a bench run) fed into one batch as requests
+        arrive: p50 / p99 time-to-result, wall clock.
 cpu_baseline the reference's own step (Imm_OPS.cpp:252-287, compiled from its sources with its own
         flags into oracle/_ref) on all host cores, on a bounded 1024 x 1024 sample.
 
@@ -42,6 +47,10 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO / "oracle"))
 
 PEAKS = REPO / "MEASURED_PEAKS.json"
+# HBM traffic per node of one FP32 step launch, dram__bytes_read.sum + dram__bytes_write.sum from one
+# ncu capture each: a launch over the 600-case batch (12.41 GB for 39 127 049 nodes) and a launch over
+# a 2048^2 drop (1239.1 MB for 4 194 304 nodes).
+TRAFFIC_B_PER_NODE = {"batch600": 12410280448 / 39127049, "single": 1239080192 / 4194304}
 HBM_FALLBACK = 6650.0
 
 
@@ -317,6 +326,29 @@ def make_case(pkg, w, prec):
     return pkg.Case(d)
 
 
+def fp64_one_at_a_time(pkg, steps=40, every=10):
+    """The plain FP64 path on the same mixed sweep, one case at a time as the reference runs it:
+    every `every`-th case of the batch mix, each stepped `steps` times alone (CUDA events around its
+    steps, creation excluded).  Aggregate MLUPS = all node updates / the sum of the case times."""
+    import torch
+    mix = batch_mix()[::every]
+    upd, ms = 0, 0.0
+    stream = torch.cuda.current_stream()
+    for c in mix:
+        case = pkg.Case(batch_desc(pkg, c, pkg.PREC_F64))
+        case.step(3, stream=stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        case.step(steps, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        upd += c["nx"] * c["nx"] * steps
+        case.close()
+    return {"value": upd / (ms * 1e-3) / 1e6, "unit": "MLUPS", "cases": len(mix), "steps": steps,
+            "workload": f"every {every}th case of the batch mix, FP64 plain, one case at a time"}
+
+
 def device_run(pkg, w, prec, steps, warmup, world, sample_clocks, local):
     """MLUPS of exactly `steps` steps, CUDA events on the launching stream, max over ranks."""
     import torch
@@ -484,6 +516,7 @@ def main():
             "roofline_frac": 608.0 * n64 * ks / (ms64 * 1e-3) / 1e9 / peak,
             "workload": "4096x4096x1 static drop R=400, P3 chi=0.5, FP64 plain (bit-identical to the reference)"}
 
+    fp64_mix = fp64_one_at_a_time(pkg) if args.workload == "batch600" else None
     e2e = None
     if not args.no_e2e:
         e2e = batch_e2e(pkg, 1001) if args.workload == "batch600" else e2e_run(pkg, single, pkg.PREC_F32, args.steps)
@@ -503,11 +536,14 @@ def main():
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "bytes_per_lu": 304.0},
+                         "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_lu": 304.0,
+                         "traffic": TRAFFIC_B_PER_NODE["batch600" if args.workload == "batch600" else "single"] * nodes,
+                         "traffic_note": "bytes per launch, from one ncu capture, scaled by nodes per launch"},
             "fp32_single_4096": single32,
             "fp64_plain": fp64,
+            "fp64_one_at_a_time_mix": fp64_mix,
             "batched_fp32_over_plain_fp64": mlups / fp64["value"],
+            "batched_fp32_over_fp64_one_at_a_time_mix": (mlups / fp64_mix["value"]) if fp64_mix else None,
             "gpu_launches": launches,
             "clocks": clocks,
             "e2e": e2e,

@@ -1,6 +1,7 @@
 // itlbm_serve -- continuous batching of case folders on one GPU.
 //
 //   itlbm_serve <spool-dir> [--budget-gb G] [--chunk K] [--fp64] [--idle-exit S] [--max-cases M]
+//               [--summary-root DIR]
 //
 // The reference runs one process per case folder (rodar_lote.py:231-243).  This server keeps one
 // batch (itlbm_batch_*) on the device and admits case folders as they arrive:
@@ -15,7 +16,9 @@
 //     or inclinada.dat, formats of the reference); at its last step or when the stop rule fires the
 //     case retires, resumo.dat is written (rodar_lote.feito's completion test) and <name>.run becomes
 //     <name>.done with its time-to-result;
-//   * <spool>/serve_stats.json keeps the count, p50 / p99 time-to-result and the aggregate MLUPS.
+//   * <spool>/serve_stats.json keeps the count, p50 / p99 time-to-result and the aggregate MLUPS;
+//   * <spool>/resumo_gota.csv and resumo_incl.csv get each retired case's row of the batch tables of
+//     analisar_lote.py (folders named relative to --summary-root), so they need no post-pass.
 // The client bin/itlbm_submit turns this into a drop-in for the Imm_OPS binary of rodar_lote.py.
 // The final VTK fields and perfil.dat are written only by itlbm_ops / itlbm_incl.
 #include <algorithm>
@@ -39,6 +42,7 @@
 
 #include "case_io.h"
 #include "case_run.h"
+#include "summary.h"
 
 using namespace itlbm_host;
 
@@ -181,13 +185,14 @@ double percentile(std::vector<double> v, double p) {
 int main(int argc, char **argv) {
     if (argc < 2) {
         std::cerr << "usage: itlbm_serve <spool-dir> [--budget-gb G] [--chunk K] [--fp64] [--idle-exit S] "
-                     "[--max-cases M]\n";
+                     "[--max-cases M] [--summary-root DIR]\n";
         return 1;
     }
     const std::string spool = argv[1];
     double budget_gb = 0, idle_exit = -1;
     int chunk = 500, max_cases = 0;
     bool fp64_default = false;
+    std::string summary_root;  // case folders are named relative to it in the batch tables
     for (int a = 2; a < argc; a++) {
         const std::string k = argv[a];
         if (k == "--budget-gb" && a + 1 < argc) budget_gb = std::atof(argv[++a]);
@@ -195,6 +200,7 @@ int main(int argc, char **argv) {
         else if (k == "--idle-exit" && a + 1 < argc) idle_exit = std::atof(argv[++a]);
         else if (k == "--max-cases" && a + 1 < argc) max_cases = std::atoi(argv[++a]);
         else if (k == "--fp64") fp64_default = true;
+        else if (k == "--summary-root" && a + 1 < argc) summary_root = argv[++a];
     }
     itlbm_batch_config cfg{};
     cfg.hbm_budget = (size_t)(budget_gb * 1e9);
@@ -277,6 +283,9 @@ int main(int argc, char **argv) {
                 else
                     j.stp->write_resumo(j.dir, j.desc.op, j.tau, j.beta, j.A, j.nx, j.theta, j.sigma_nominal,
                                         steps, mlups);
+                // the analisar_lote.py tables, one row per retired case
+                append_summary_row(join(spool, j.drop ? "resumo_gota.csv" : "resumo_incl.csv"), j.dir, summary_root,
+                                   !j.drop);
                 std::ostringstream done;
                 done << std::setprecision(10) << (e.kind == ITLBM_EV_DONE ? "estavel" : "instavel") << " " << steps
                      << " " << latency << "\n";

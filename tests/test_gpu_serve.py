@@ -23,7 +23,8 @@ def submit(d, spool, prec="fp64"):
 def test_served_equals_alone_and_overlaps(tmp_path):
     spool = tmp_path / "spool"
     spool.mkdir()
-    server = subprocess.Popen([str(BIN / "itlbm_serve"), str(spool), "--idle-exit", "3", "--chunk", "250"],
+    server = subprocess.Popen([str(BIN / "itlbm_serve"), str(spool), "--idle-exit", "3", "--chunk", "250",
+                               "--summary-root", str(tmp_path)],
                               stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
     try:
         cases = [("P3 0.5", 0.225, 40, 1501, None), ("F2", 0.1, 56, 1200, None), ("F3 1.569988", 0.1, 48, 999, None),
@@ -60,6 +61,17 @@ def test_served_equals_alone_and_overlaps(tmp_path):
         ra = (dirs[k] / "resumo.dat").read_text().splitlines()
         rb = (alone / "resumo.dat").read_text().splitlines()
         assert ra[0] == rb[0] and ra[1].split()[:-1] == rb[1].split()[:-1]  # all but the MLUPS column
+    # the analisar_lote.py table rows, appended as each case retired
+    import csv
+    with open(spool / "resumo_gota.csv", newline="") as f:
+        gota = {r["pasta"]: r for r in csv.DictReader(f)}
+    with open(spool / "resumo_incl.csv", newline="") as f:
+        incl = {r["pasta"]: r for r in csv.DictReader(f)}
+    n_strips = sum(1 for c in cases if c[4])
+    assert len(gota) == len(cases) - n_strips and len(incl) == n_strips
+    for k, c in enumerate(cases):
+        row = (incl if c[4] else gota)[f"s{k}"]
+        assert row["rotulo"] == f"s{k}" and row["estado"] == "estavel"
     import json
     stats = json.loads((spool / "serve_stats.json").read_text())
     assert stats["completed"] == len(cases) and stats["invalid"] == 1 and stats["p99_s"] > 0

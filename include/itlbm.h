@@ -65,7 +65,12 @@ typedef struct itlbm_operador {
 
 /* ---- case description --------------------------------------------------------------------- */
 enum { ITLBM_GEOM_DROP = 0, ITLBM_GEOM_STRIP = 1 };
-enum { ITLBM_PREC_F64 = 0, ITLBM_PREC_F32 = 1 };
+/* ITLBM_PREC_F32_FOLD (no counterpart in the reference): FP32 storage of the nine in-plane classes of
+ * D3Q19 per colour (144 instead of 304 bytes per update).  For the one-node slab the class sums evolve
+ * exactly as the 19 populations do (up to rounding); read_pops returns each class split among its
+ * members by weight, so the per-direction minima and counts of negative populations and the P_zz of the
+ * strip's sigma_pop are those of the split. */
+enum { ITLBM_PREC_F64 = 0, ITLBM_PREC_F32 = 1, ITLBM_PREC_F32_FOLD = 2 };
 
 typedef struct itlbm_case_desc {
     int    nx, ny;            /* box nx x ny x 1, all fluid, periodic                           */
@@ -196,6 +201,16 @@ int  itlbm_case_write_pops(itlbm_case *c, const double *fR, const double *fB);
 int  itlbm_case_read_fields(itlbm_case *c, double *rho_R, double *rho_B, double *ux, double *uy,
                             double *uz, double *force);
 
+/* Sync.  Case snapshots: the reference restarts an interrupted batch from step 0 (rodar_lote.py:5-7);
+ * these save a case (its description, its step count and its populations at the top of its next
+ * step, in its own precision) and restore it on the current device.  Stepping a restored case gives
+ * the same bits the saved case would have given.  The kept force (ITLBM_STEP_KEEP_AUX) is not saved:
+ * the next step of a restored class-F case must keep it before a diagnostic. */
+int  itlbm_case_save(itlbm_case *c, const char *path);
+int  itlbm_case_load(const char *path, itlbm_case **out);
+/* The description and step count stored in a snapshot, without touching the device. */
+int  itlbm_snapshot_info(const char *path, itlbm_case_desc *desc, long long *steps);
+
 /* ---- batches: many cases stepped together ------------------------------------------------- */
 /* The batched form of the loop Imm_OPS.cpp:246-372 / Imm_INCL.cpp:358-442 for many independent
  * cases, replacing the process pool of rodar_lote.py (rodar_lote.py:231-243, :300-318).  Admitted
@@ -240,6 +255,12 @@ void itlbm_batch_destroy(itlbm_batch *b);
 /* Queues a case of n_steps steps.  It is admitted at the next advance when its state fits the HBM
  * budget and a slot is free (ITLBM_E_ADMISSION if it can never fit).  `tag` comes back in events. */
 int  itlbm_batch_submit(itlbm_batch *b, const itlbm_case_desc *d, int n_steps, long long tag);
+/* Batch snapshots (see itlbm_case_save): itlbm_batch_save writes the active case `tag` as it stands
+ * between two advances; itlbm_batch_submit_saved queues a case that starts from a snapshot (of a
+ * batch or of a single case) and runs on to step n_steps (its diagnostics keep the absolute step
+ * numbers). */
+int  itlbm_batch_save(itlbm_batch *b, long long tag, const char *path);
+int  itlbm_batch_submit_saved(itlbm_batch *b, const char *path, int n_steps, long long tag);
 /* One round: admit, run one graph replay (every active case advances to its next diagnostic step
  * or by `chunk` steps), run the diagnostics that fell due, retire finished and unstable cases.
  * Returns the number of events now waiting (>= 0) or an error code. */

@@ -24,7 +24,7 @@ N_ANG = 256
 # operator codes (OP_P1..OP_F3, Operadores_tensao.cpp:45-49)
 OP_P1, OP_P3, OP_F1, OP_F2, OP_F3 = 1, 3, 11, 12, 13
 GEOM_DROP, GEOM_STRIP = 0, 1
-PREC_F64, PREC_F32 = 0, 1
+PREC_F64, PREC_F32, PREC_F32_FOLD = 0, 1, 2
 STEP_KEEP_AUX = 1
 
 ERRORS = {
@@ -89,6 +89,11 @@ class StripDiag(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SnapHeader(C.Structure):
+    """Header of a case snapshot (itlbm_case_save / itlbm_batch_save)."""
+    _fields_ = [("magic", C.c_char * 8), ("version", C.c_int), ("desc", CaseDesc), ("steps", C.c_longlong)]
+
+
 class BatchConfig(C.Structure):
     _fields_ = [("hbm_budget", C.c_size_t), ("max_cases", C.c_int), ("chunk", C.c_int),
                 ("diag_every", C.c_int), ("ctas_per_sm", C.c_int)]
@@ -145,6 +150,11 @@ def lib():
         "itlbm_case_read_pops": (C.c_int, [vp, C.c_int, dp, dp]),
         "itlbm_case_write_pops": (C.c_int, [vp, dp, dp]),
         "itlbm_case_read_fields": (C.c_int, [vp, dp, dp, dp, dp, dp, dp]),
+        "itlbm_case_save": (C.c_int, [vp, C.c_char_p]),
+        "itlbm_case_load": (C.c_int, [C.c_char_p, P(vp)]),
+        "itlbm_snapshot_info": (C.c_int, [C.c_char_p, P(CaseDesc), P(C.c_longlong)]),
+        "itlbm_batch_save": (C.c_int, [vp, C.c_longlong, C.c_char_p]),
+        "itlbm_batch_submit_saved": (C.c_int, [vp, C.c_char_p, C.c_int, C.c_longlong]),
         "itlbm_batch_create": (C.c_int, [P(BatchConfig), P(vp)]),
         "itlbm_batch_destroy": (None, [vp]),
         "itlbm_batch_submit": (C.c_int, [vp, P(CaseDesc), C.c_int, C.c_longlong]),
@@ -249,6 +259,23 @@ class Case:
               "itlbm_case_diag_drop")
         return out
 
+    def save(self, path):
+        check(lib().itlbm_case_save(self._h, str(path).encode()), "itlbm_case_save")
+
+    @classmethod
+    def load(cls, path):
+        """A case restored from a snapshot written by save() (or by Batch.save)."""
+        hd = SnapHeader()
+        with open(path, "rb") as f:
+            C.memmove(C.byref(hd), f.read(C.sizeof(SnapHeader)), C.sizeof(SnapHeader))
+        h = C.c_void_p()
+        check(lib().itlbm_case_load(str(path).encode(), C.byref(h)), "itlbm_case_load")
+        c = cls.__new__(cls)
+        c.desc = hd.desc
+        c.n = hd.desc.nx * hd.desc.ny
+        c._h = h
+        return c
+
     def diag_drop_static(self, step, x_ini=None, y_ini=None, stream=None) -> DropDiag:
         """diag_drop on the library's fixed device scratch (no allocation; cases of at most
         512 x 512 nodes; concurrent calls on one device race)."""
@@ -314,6 +341,12 @@ class Batch:
 
     def submit(self, d: CaseDesc, n_steps: int, tag: int):
         check(lib().itlbm_batch_submit(self._h, C.byref(d), n_steps, tag), "itlbm_batch_submit")
+
+    def save(self, tag, path):
+        check(lib().itlbm_batch_save(self._h, tag, str(path).encode()), "itlbm_batch_save")
+
+    def submit_saved(self, path, n_steps, tag):
+        check(lib().itlbm_batch_submit_saved(self._h, str(path).encode(), n_steps, tag), "itlbm_batch_submit_saved")
 
     def advance(self):
         r = lib().itlbm_batch_advance(self._h, None)

@@ -60,6 +60,7 @@ cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntil
                         const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
                         cudaStream_t s) {
     if (prec == ITLBM_PREC_F64) return launch_step_f64(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
+    if (prec == ITLBM_PREC_F32_FOLD) return launch_step_fold(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
     return march ? launch_march_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s)
                  : launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
 }
@@ -211,7 +212,7 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
         return fail(ITLBM_E_ARG, "box size out of range");
     if (!op_valid(d->op.tipo)) return fail(ITLBM_E_ARG, "unknown operator");
     if (!(d->tau > 0.0) || !std::isfinite(d->tau)) return fail(ITLBM_E_ARG, "tau must be > 0");
-    if (d->precision != ITLBM_PREC_F64 && d->precision != ITLBM_PREC_F32)
+    if (!prec_valid(d->precision))
         return fail(ITLBM_E_ARG, "unknown precision");
     if (d->geometry == ITLBM_GEOM_STRIP) {
         if (d->nx != d->ny) return fail(ITLBM_E_ARG, "strip needs a square box (Imm_INCL.cpp:243)");
@@ -232,8 +233,8 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
     h.chunk_len = INT_MAX;
     h.aux_at_end = 0;
     fill_params(h, d->op, d->tau, d->A_fact, d->beta, d->rho_B > 0 ? d->rho_B : 1.0);
-    const size_t elem = d->precision == ITLBM_PREC_F64 ? 8 : 4;
-    const size_t per_buf = (size_t)2 * NV * h.stride * elem;
+    const size_t elem = elem_of(d->precision);
+    const size_t per_buf = (size_t)2 * planes_of(d->precision) * h.stride * elem;
     if ((e = cudaMalloc(&c->mem, 2 * per_buf)) != cudaSuccess) {
         itlbm_case_destroy(c);
         return cuda_fail(e, "cudaMalloc(state)");
@@ -313,6 +314,41 @@ int itlbm_case_sync(itlbm_case *c) {
 }
 
 long long itlbm_case_steps_done(const itlbm_case *c) { return c ? c->steps : -1; }
+
+int itlbm_case_save(itlbm_case *c, const char *path) {
+    if (!c || !path) return fail(ITLBM_E_ARG, "NULL argument");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaDeviceSynchronize();  // steps may have gone to another stream
+    if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+    return snap_write(path, c->desc, c->steps, c->host, c->host.buf[c->steps & 1]);
+}
+
+int itlbm_snapshot_info(const char *path, itlbm_case_desc *desc, long long *steps) {
+    if (!path || !desc || !steps) return fail(ITLBM_E_ARG, "NULL argument");
+    SnapHeader hd;
+    const int r = snap_read_header(path, hd);
+    if (r) return r;
+    *desc = hd.desc;
+    *steps = hd.steps;
+    return ITLBM_OK;
+}
+
+int itlbm_case_load(const char *path, itlbm_case **out) {
+    if (!path || !out) return fail(ITLBM_E_ARG, "NULL argument");
+    *out = nullptr;
+    SnapHeader hd;
+    int r = snap_read_header(path, hd);
+    if (r) return r;
+    itlbm_case *c = nullptr;
+    if ((r = itlbm_case_create(&hd.desc, &c)) != ITLBM_OK) return r;
+    c->steps = hd.steps;
+    if ((r = snap_read_state(path, c->host, c->host.buf[c->steps & 1])) != ITLBM_OK) {
+        itlbm_case_destroy(c);
+        return r;
+    }
+    *out = c;
+    return ITLBM_OK;
+}
 
 static int ensure_diag(itlbm_case *c) {
     cudaError_t e = diag_alloc(c->diag, c->host.nx, c->host.ny);

@@ -37,6 +37,8 @@ struct Pending {
     int n_steps;
     long long tag;
     double t_submit;
+    std::string snapshot;  // restore from this file instead of the initial state
+    long long start = 0;   // its step count
 };
 
 struct Active {
@@ -57,10 +59,15 @@ struct Active {
 size_t case_bytes(const itlbm_case_desc &d, bool &need_aux) {
     const long long pitch = (d.nx + 31) / 32 * 32;
     const long long stride = pitch * d.ny;
-    const size_t elem = d.precision == ITLBM_PREC_F64 ? 8 : 4;
+    const size_t elem = elem_of(d.precision);
     need_aux = d.op.tipo >= ITLBM_OP_F1 || d.geometry == ITLBM_GEOM_STRIP;
-    return (size_t)2 * 2 * NV * stride * elem + (need_aux ? (size_t)4 * stride * 8 : 0);
+    return (size_t)2 * 2 * planes_of(d.precision) * stride * elem + (need_aux ? (size_t)4 * stride * 8 : 0);
 }
+
+// the work tables, one per storage form: [0] FP64, [1] FP32, [2] FP32 fold
+constexpr int NTAB = 3;
+int table_of(int prec) { return prec == ITLBM_PREC_F64 ? 0 : (prec == ITLBM_PREC_F32 ? 1 : 2); }
+int prec_of_table(int p) { return p == 0 ? ITLBM_PREC_F64 : (p == 1 ? ITLBM_PREC_F32 : ITLBM_PREC_F32_FOLD); }
 
 const double U_LIMITE = 0.4;  // Imm_OPS.cpp:45
 
@@ -75,11 +82,11 @@ struct itlbm_batch {
     std::vector<int> free_slots;
     std::vector<CaseDev> h_cases;
     CaseDev *d_cases = nullptr;
-    TileRef *d_tiles[2] = {nullptr, nullptr};  // [0] FP64 cases, [1] FP32 cases
-    int tiles_cap[2] = {0, 0};
+    TileRef *d_tiles[NTAB] = {};  // per storage form (table_of)
+    int tiles_cap[NTAB] = {};
     int *d_ntiles = nullptr;
     bool tables_dirty = true;
-    int grid[2] = {0, 0};
+    int grid[NTAB] = {};
     bool march = false;  // FP32 cases run the marching kernel
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -104,16 +111,16 @@ struct itlbm_batch {
 namespace {
 
 int upload_tables(itlbm_batch *b) {
-    std::vector<TileRef> t[2];
+    std::vector<TileRef> t[NTAB];
     for (Active *a : b->slots) {
         if (!a) continue;
         const CaseDev &c = b->h_cases[a->slot];
-        const int p = a->desc.precision == ITLBM_PREC_F64 ? 0 : 1;
+        const int p = table_of(a->desc.precision);
         const int n = case_items(c);
         for (int k = 0; k < n; k++) t[p].push_back(TileRef{a->slot, k});
     }
-    int n[2];
-    for (int p = 0; p < 2; p++) {
+    int n[NTAB];
+    for (int p = 0; p < NTAB; p++) {
         n[p] = (int)t[p].size();
         if (n[p] > b->tiles_cap[p]) {
             if (b->d_tiles[p]) cudaFree(b->d_tiles[p]);
@@ -128,9 +135,9 @@ int upload_tables(itlbm_batch *b) {
         }
     }
     if (b->cfg.ctas_per_sm <= 0)
-        for (int p = 0; p < 2; p++) b->grid[p] = n[p];
+        for (int p = 0; p < NTAB; p++) b->grid[p] = n[p];
     // the graph reads the table pointers it was captured with: keep them, or re-capture
-    cudaError_t e = cudaMemcpyAsync(b->d_ntiles, n, sizeof(int) * 2, cudaMemcpyHostToDevice, b->stream);
+    cudaError_t e = cudaMemcpyAsync(b->d_ntiles, n, sizeof(int) * NTAB, cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "work table length");
     return cudaStreamSynchronize(b->stream) == cudaSuccess ? ITLBM_OK : cuda_fail(cudaGetLastError(), "sync");
 }
@@ -144,8 +151,9 @@ int capture_graph(itlbm_batch *b) {
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "begin capture");
     for (int k = 0; k < b->cfg.chunk; k++) {
-        launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, false, b->stream);
-        launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->march, b->stream);
+        for (int p = 0; p < NTAB; p++)
+            launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
+                        p == 1 && b->march, b->stream);
     }
     e = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) return cuda_fail(e, "end capture");
@@ -182,8 +190,8 @@ int admit(itlbm_batch *b) {
         CaseDev h{};
         case_layout(h, d.nx, d.ny, d.precision, b->march);
         fill_params(h, d.op, d.tau, d.A_fact, d.beta, d.rho_B > 0 ? d.rho_B : 1.0);
-        const size_t elem = d.precision == ITLBM_PREC_F64 ? 8 : 4;
-        const size_t per_buf = (size_t)2 * NV * h.stride * elem;
+        const size_t elem = elem_of(d.precision);
+        const size_t per_buf = (size_t)2 * planes_of(d.precision) * h.stride * elem;
         cudaError_t e = cudaMalloc(&a->mem, 2 * per_buf);
         if (e == cudaSuccess && need_aux) e = cudaMalloc(&a->aux, sizeof(double) * 4 * (size_t)h.stride);
         if (e != cudaSuccess) {
@@ -208,8 +216,16 @@ int admit(itlbm_batch *b) {
         b->h_cases[slot] = h;
         // on the batch stream, which is not ordered after the legacy stream's copies
         e = cudaMemcpyAsync(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream);
-        if (e == cudaSuccess) e = launch_init(h, b->d_cases + slot, d, b->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "admission");
+        if (p.snapshot.empty()) {
+            if (e == cudaSuccess) e = launch_init(h, b->d_cases + slot, d, b->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "admission");
+        } else {
+            if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "admission");
+            const int r = snap_read_state(p.snapshot.c_str(), h, h.buf[0]);
+            if (r) return r;
+            a->next_step = (int)p.start;
+        }
         b->hbm_used += bytes;
         b->tables_dirty = true;
         b->pending.pop_front();
@@ -248,7 +264,7 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
     // launch shape: one CTA per tile of the work table (the grid follows the table and the graph is
     // re-captured when it changes), or, with ctas_per_sm > 0, that many persistent CTAs per SM
     // striding over the table
-    for (int p = 0; p < 2; p++) b->grid[p] = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm * b->sms : 0;
+    for (int p = 0; p < NTAB; p++) b->grid[p] = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm * b->sms : 0;
     const int M = b->cfg.max_cases;
     b->slots.assign(M, nullptr);
     for (int s = M - 1; s >= 0; s--) b->free_slots.push_back(s);
@@ -257,17 +273,17 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
     b->h_strip.resize(M);
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_cases, sizeof(CaseDev) * M)) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_ntiles, sizeof(int) * 2)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_ntiles, sizeof(int) * NTAB)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_drop, sizeof(itlbm_drop_diag) * M)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_strip, sizeof(itlbm_strip_diag) * M)) != cudaSuccess) {
         itlbm_batch_destroy(b);
         return cuda_fail(e, "batch allocation");
     }
     cudaMemsetAsync(b->d_cases, 0, sizeof(CaseDev) * M, b->stream);
-    cudaMemsetAsync(b->d_ntiles, 0, sizeof(int) * 2, b->stream);
+    cudaMemsetAsync(b->d_ntiles, 0, sizeof(int) * NTAB, b->stream);
     cudaStreamSynchronize(b->stream);
     // work tables with room for a first batch, so the graph can be captured with their addresses
-    for (int p = 0; p < 2; p++) {
+    for (int p = 0; p < NTAB; p++) {
         b->tiles_cap[p] = 1 << 16;
         if ((e = cudaMalloc(&b->d_tiles[p], sizeof(TileRef) * b->tiles_cap[p])) != cudaSuccess) {
             itlbm_batch_destroy(b);
@@ -298,7 +314,7 @@ void itlbm_batch_destroy(itlbm_batch *b) {
         }
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->d_cases) cudaFree(b->d_cases);
-    for (int p = 0; p < 2; p++)
+    for (int p = 0; p < NTAB; p++)
         if (b->d_tiles[p]) cudaFree(b->d_tiles[p]);
     if (b->d_ntiles) cudaFree(b->d_ntiles);
     if (b->d_drop) cudaFree(b->d_drop);
@@ -310,17 +326,42 @@ void itlbm_batch_destroy(itlbm_batch *b) {
     delete b;
 }
 
+int itlbm_batch_submit_saved(itlbm_batch *b, const char *path, int n_steps, long long tag) {
+    if (!b || !path) return fail(ITLBM_E_ARG, "bad argument");
+    SnapHeader hd;
+    int r = snap_read_header(path, hd);
+    if (r) return r;
+    if (n_steps <= hd.steps) return fail(ITLBM_E_ARG, "the snapshot is already at or past n_steps");
+    if ((r = itlbm_batch_submit(b, &hd.desc, n_steps, tag)) != ITLBM_OK) return r;
+    b->pending.back().snapshot = path;
+    b->pending.back().start = hd.steps;
+    return ITLBM_OK;
+}
+
+int itlbm_batch_save(itlbm_batch *b, long long tag, const char *path) {
+    if (!b || !path) return fail(ITLBM_E_ARG, "bad argument");
+    cudaSetDevice(b->device);
+    for (Active *a : b->slots) {
+        if (!a || a->tag != tag) continue;
+        cudaError_t e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+        const CaseDev &h = b->h_cases[a->slot];
+        return snap_write(path, a->desc, a->next_step, h, h.buf[a->parity]);
+    }
+    return fail(ITLBM_E_ARG, "no active case with this tag");
+}
+
 int itlbm_batch_submit(itlbm_batch *b, const itlbm_case_desc *d, int n_steps, long long tag) {
     if (!b || !d || n_steps < 1) return fail(ITLBM_E_ARG, "bad argument");
     if (d->nx < 1 || d->ny < 1 || !(d->tau > 0.0) ||
-        (d->precision != ITLBM_PREC_F64 && d->precision != ITLBM_PREC_F32) ||
+        !prec_valid(d->precision) ||
         (d->geometry != ITLBM_GEOM_DROP && d->geometry != ITLBM_GEOM_STRIP) ||
         (d->geometry == ITLBM_GEOM_STRIP && (d->nx != d->ny || (d->p == 0 && d->q == 0))))
         return fail(ITLBM_E_ARG, "invalid case description");
     bool need_aux;
     if (case_bytes(*d, need_aux) > b->cfg.hbm_budget)
         return fail(ITLBM_E_ADMISSION, "case larger than the batch's HBM budget");
-    b->pending.push_back(Pending{*d, n_steps, tag, b->now()});
+    b->pending.push_back(Pending{*d, n_steps, tag, b->now(), std::string(), 0});
     return ITLBM_OK;
 }
 
@@ -352,11 +393,17 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
                                     cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "case table upload");
     if (b->tables_dirty) {
-        TileRef *old0 = b->d_tiles[0], *old1 = b->d_tiles[1];
-        const int g0 = b->grid[0], g1 = b->grid[1];
+        TileRef *old[NTAB];
+        int g[NTAB];
+        for (int p = 0; p < NTAB; p++) {
+            old[p] = b->d_tiles[p];
+            g[p] = b->grid[p];
+        }
         r = upload_tables(b);
         if (r) return r;
-        if (old0 != b->d_tiles[0] || old1 != b->d_tiles[1] || g0 != b->grid[0] || g1 != b->grid[1]) {
+        bool changed = false;
+        for (int p = 0; p < NTAB; p++) changed = changed || old[p] != b->d_tiles[p] || g[p] != b->grid[p];
+        if (changed) {
             r = capture_graph(b);
             if (r) return r;
         }
@@ -368,8 +415,9 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         if (e != cudaSuccess) return cuda_fail(e, "graph launch");
     } else {
         for (int k = 0; k < K; k++) {
-            launch_step(b->d_cases, b->d_tiles[0], 0, b->d_ntiles + 0, b->grid[0], k, -1, ITLBM_PREC_F64, false, b->stream);
-            launch_step(b->d_cases, b->d_tiles[1], 0, b->d_ntiles + 1, b->grid[1], k, -1, ITLBM_PREC_F32, b->march, b->stream);
+            for (int p = 0; p < NTAB; p++)
+                launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
+                            p == 1 && b->march, b->stream);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "step launches");
     }

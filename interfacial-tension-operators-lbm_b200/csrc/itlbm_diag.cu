@@ -46,7 +46,7 @@ __device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int 
             fR[i] = d[(long long)i * c.stride + o];
             fB[i] = d[(long long)(NV + i) * c.stride + o];
         });
-    } else {
+    } else if (c.prec == ITLBM_PREC_F32) {
         const float *d = (const float *)c.buf[cur];
         sfor<0, NV>([&](auto I) {
             constexpr int i = decltype(I)::value;
@@ -56,6 +56,21 @@ __device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int 
             const double e = d[(long long)i * c.stride + o];
             const double dd = d[(long long)(NV + i) * c.stride + o];
             const double f = wgt<double>(i) * c.rho0 + e;
+            fR[i] = 0.5 * (f + dd);
+            fB[i] = 0.5 * (f - dd);
+        });
+    } else {  // fold: class K was pushed to x + e_K, the same in-plane shift as each of its members;
+              // the class is split among its members by weight (exact for every moment)
+        const float *d = (const float *)c.buf[cur];
+        sfor<0, NV>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            constexpr int K = fold_class(i);
+            const int xs = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
+            const int ys = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
+            const long long o = (long long)ys * c.pitch + xs;
+            const double share = wgt<double>(i) / wk<double>(K);
+            const double f = (wk<double>(K) * c.rho0 + d[(long long)K * c.stride + o]) * share;
+            const double dd = d[(long long)(NK + K) * c.stride + o] * share;
             fR[i] = 0.5 * (f + dd);
             fB[i] = 0.5 * (f - dd);
         });

@@ -50,6 +50,39 @@ __host__ __device__ constexpr T wgt(int i) {
     return i == 0 ? T(1.) / T(3.) : (i < 7 ? T(1.) / T(18.) : T(1.) / T(36.));
 }
 
+// In-plane fold of D3Q19 for the one-node slab (FP32 fold storage, ITLBM_PREC_F32_FOLD).  With one
+// node in z and periodic z, a direction with c_z = +-1 streams to the same (x, y) as its in-plane
+// projection, and a z-symmetric state (every initial state here) stays z-symmetric, so the 19
+// populations of a colour group into nine classes of equal in-plane velocity e_K whose sums evolve
+// exactly as a D2Q9 lattice with weights W_K = sum of the members' w_i (4/9, 1/9, 1/36):
+//   K0 {0, 5, 6}  K1 +x {1, 11, 13}  K2 -x {2, 12, 14}  K3 +y {3, 16, 18}  K4 -y {4, 15, 17}
+//   K5 {7}  K6 {8}  K7 {9}  K8 {10}            (classes 2m - 1 and 2m are opposite, m = 1..4)
+constexpr int NK = 9;
+__host__ __device__ constexpr int fold_class(int i) {
+    constexpr int t[NV] = {0, 1, 2, 3, 4, 0, 0, 5, 6, 7, 8, 1, 2, 1, 2, 4, 3, 4, 3};
+    return t[i];
+}
+__host__ __device__ constexpr int kx(int K) {
+    constexpr int t[NK] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+    return t[K];
+}
+__host__ __device__ constexpr int ky(int K) {
+    constexpr int t[NK] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
+    return t[K];
+}
+__host__ __device__ constexpr int kk(int K) { return kx(K) * kx(K) + ky(K) * ky(K); }
+template <class T>
+__host__ __device__ constexpr T wk(int K) {
+    return K == 0 ? T(4.) / T(9.) : (K < 5 ? T(1.) / T(9.) : T(1.) / T(36.));
+}
+
+// storage planes per colour and bytes per element of a precision
+__host__ __device__ constexpr int planes_of(int prec) { return prec == ITLBM_PREC_F32_FOLD ? NK : NV; }
+__host__ __device__ constexpr int elem_of(int prec) { return prec == ITLBM_PREC_F64 ? 8 : 4; }
+__host__ __device__ constexpr bool prec_valid(int prec) {
+    return prec == ITLBM_PREC_F64 || prec == ITLBM_PREC_F32 || prec == ITLBM_PREC_F32_FOLD;
+}
+
 // Compile-time loop: f(std::integral_constant<int, i>) for i in [B, E).
 template <int B, int E, class F>
 __host__ __device__ __forceinline__ void sfor(F &&f) {
@@ -96,6 +129,8 @@ cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int 
                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
 cudaError_t launch_step_f32(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
+cudaError_t launch_step_fold(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
+                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
 int step_occupancy_f64();
 int step_occupancy_f32();
 int step_occupancy(int prec);
@@ -157,6 +192,18 @@ cudaError_t launch_diag_strip(const CaseDev *c_dev, const CaseDev &c, DiagScratc
 cudaError_t launch_fields(const CaseDev *c_dev, const CaseDev &c, int cur, bool use_force,
                           double *rho_R, double *rho_B, double *ux, double *uy, double *uz,
                           cudaStream_t st);
+
+// ---- case snapshots (itlbm_snapshot.cu) ------------------------------------------------------
+struct SnapHeader {
+    char magic[8];            // "ITLBMST1"
+    int version;              // 1
+    itlbm_case_desc desc;
+    long long steps;          // steps done: the state is the one at the top of step `steps`
+};
+// `state` is the device buffer holding the state at the top of the next step.
+int snap_write(const char *path, const itlbm_case_desc &d, long long steps, const CaseDev &h, const void *state);
+int snap_read_header(const char *path, SnapHeader &hd);
+int snap_read_state(const char *path, const CaseDev &h, void *state);
 
 // ---- error reporting -------------------------------------------------------------------------
 void set_error(const std::string &msg);

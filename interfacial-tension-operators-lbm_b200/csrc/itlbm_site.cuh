@@ -359,6 +359,146 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
     rc.gz = gmz;
 }
 
+// ---------------------------------------------------------------------------------------------
+// FP32 fold: the nine in-plane classes of D3Q19 (see itlbm_internal.h), by opposite pairs
+// (classes 2m - 1 and 2m, m = 1..4).  Every term of colisao_comum is linear in the populations of
+// a class member or depends only on the moments, and members of a class share c . u, c . F and c . g
+// (u_z = F_z = g_z = 0), so the class sums follow from class quantities:
+//   sum w_i = W_K;  sum B_i = B0 + 2 B1 (K0), B1 + 2 B2 (axes), B2 (diagonals);
+//   sum w_i / |c_i| (recolouring) = (1 + 1/sqrt 2) / 18 (axes), 1 / (36 sqrt 2) (diagonals).
+// ---------------------------------------------------------------------------------------------
+template <int K, class T>
+__device__ __forceinline__ T kdot(T a, T b) {  // e_K . (a, b)
+    if constexpr (kx(K) == 0) return ky(K) > 0 ? b : -b;
+    else if constexpr (ky(K) == 0) return kx(K) > 0 ? a : -a;
+    else {
+        const T s = kx(K) > 0 ? a : -a;
+        return ky(K) > 0 ? s + b : s - b;
+    }
+}
+
+struct RecolourFold {
+    float phi, k1, k2, gx, gy;
+    bool skip;
+};
+
+// d_K and d_{K+1} of the class pair (K, K + 1), K odd, from the post-collision e_K, e_{K+1}.
+template <int K>
+__device__ __forceinline__ void split_fold_pair(const RecolourFold &r, float eK, float eJ, float rho0, float &dK,
+                                                float &dJ) {
+    const float wr = wk<float>(K) * rho0;
+    const float A = kdot<K>(r.gx, r.gy) * (kk(K) == 1 ? r.k1 : r.k2);
+    dK = fmaf(r.phi, wr + eK, -A);
+    dJ = fmaf(r.phi, wr + eJ, A);
+}
+
+// e_K = F_K - W_K rho0 of the nine classes in, post-collision out; drho = sum e_K, D = sum d_K.
+template <bool FORCE>
+__device__ __forceinline__ void collide_fold(float (&e)[NK], float drho, float D, float gmx, float gmy,
+                                             float Fx, float Fy, const CaseDev &c, RecolourFold &rc) {
+    const float rho0 = (float)c.rho0;
+    const float rho = rho0 + drho;
+    rc.skip = !(rho > 1.0e-30f);
+    if (rc.skip) return;
+    const float inv_rho = 1.0f / rho;
+    const float phi = D * inv_rho;
+    float ax = 0.f, ay = 0.f;
+    if constexpr (FORCE) {
+        ax = Fx * inv_rho;
+        ay = Fy * inv_rho;
+    }
+    float jx = 0.f, jy = 0.f;
+    sfor<0, 4>([&](auto M) {
+        constexpr int K = 2 * decltype(M)::value + 1;
+        const float p = e[K] - e[K + 1];
+        if constexpr (kx(K) == 1) jx += p;
+        if constexpr (kx(K) == -1) jx -= p;
+        if constexpr (ky(K) == 1) jy += p;
+        if constexpr (ky(K) == -1) jy -= p;
+    });
+    const float vx = fmaf(jx, inv_rho, 0.5f * ax), vy = fmaf(jy, inv_rho, 0.5f * ay);
+    const float usq15 = 1.5f * (vx * vx + vy * vy);
+    const float inv_tau = (float)c.inv_tau;
+    const float rho3 = 3.0f * rho;
+    const float Frx = ax * rho, Fry = ay * rho;
+    const float vF = Frx * vx + Fry * vy;
+    const float fac3 = 3.0f * (float)c.src_factor;
+    sfor<0, 4>([&](auto M) {
+        constexpr int K = 2 * decltype(M)::value + 1;
+        constexpr float W = wk<float>(K);
+        const float cu = kdot<K>(vx, vy);
+        const float sym = W * fmaf(rho, fmaf(4.5f * cu, cu, -usq15), drho);
+        const float asym = (W * rho3) * cu;
+        float eK = fmaf((sym + asym) - e[K], inv_tau, e[K]);
+        float eJ = fmaf((sym - asym) - e[K + 1], inv_tau, e[K + 1]);
+        if constexpr (FORCE) {
+            const float cF = kdot<K>(Frx, Fry);
+            const float P = fmaf(3.0f * cF, cu, -vF);
+            eK = fmaf(fac3 * W, P + cF, eK);
+            eJ = fmaf(fac3 * W, P - cF, eJ);
+        }
+        e[K] = eK;
+        e[K + 1] = eJ;
+    });
+    const float mod2 = gmx * gmx + gmy * gmy;
+    const float mod = sqrtf(mod2);
+    if constexpr (!FORCE) {
+        const float A = (float)c.A;
+        if (!(mod2 <= 1.0e-30f || A == 0.0f)) {
+            const float inv2 = 1.0f / mod2;
+            const float amod = A * mod;
+            const float Bax = (float)(c.B1 + 2.0 * c.B2), Bdg = (float)c.B2;
+            sfor<0, 4>([&](auto M) {
+                constexpr int K = 2 * decltype(M)::value + 1;
+                constexpr float W = wk<float>(K);
+                const float cg = kdot<K>(gmx, gmy);
+                const float om = amod * fmaf(W * cg, cg * inv2, -(kk(K) == 1 ? Bax : Bdg));
+                e[K] += om;
+                e[K + 1] += om;
+            });
+        }
+    }
+    e[0] = drho - (((e[1] + e[2]) + (e[3] + e[4])) + ((e[5] + e[6]) + (e[7] + e[8])));
+    const float fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
+    const float inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
+    rc.phi = phi;
+    rc.k1 = fat2 * ((1.0f + 0.70710678118654752f) / 18.0f) * inv_mod;
+    rc.k2 = fat2 * (0.70710678118654752f / 36.0f) * inv_mod;
+    rc.gx = gmx;
+    rc.gy = gmy;
+}
+
+// Mediator momentum sum_K e_K W_K 3 phi(x - e_K) of the fold; the isotropic gradient is its negative.
+template <class P>
+__device__ __forceinline__ void mediator_grad_fold(P phi, float &gx, float &gy) {
+    float ax = 0.f, ay = 0.f;
+    sfor<0, 4>([&](auto M) {
+        constexpr int K = 2 * decltype(M)::value + 1;
+        constexpr float w3 = 3.0f * wk<float>(K);
+        const float dphi = w3 * (phi(-kx(K), -ky(K)) - phi(kx(K), ky(K)));
+        if constexpr (kx(K) == 1) ax += dphi;
+        if constexpr (kx(K) == -1) ax -= dphi;
+        if constexpr (ky(K) == 1) ay += dphi;
+        if constexpr (ky(K) == -1) ay -= dphi;
+    });
+    gx = ax;
+    gy = ay;
+}
+// F3 chemical potential, lap = 6 sum_K W_K (phi(x + e_K) - phi)
+template <class P>
+__device__ __forceinline__ float chem_pot_fold(P phi, float kf, float bf) {
+    const float ph = phi(0, 0);
+    float l1 = 0.f, l2 = 0.f;
+    sfor<0, 4>([&](auto M) {
+        constexpr int K = 2 * decltype(M)::value + 1;
+        const float s = phi(kx(K), ky(K)) + phi(-kx(K), -ky(K));
+        if constexpr (kk(K) == 1) l1 += s;
+        else l2 += s;
+    });
+    const float lap = 6.0f * (fmaf(-4.0f, ph, l1) * (1.0f / 9.0f) + fmaf(-4.0f, ph, l2) * (1.0f / 36.0f));
+    return 4.0f * bf * ph * (ph * ph - 1.0f) - kf * lap;
+}
+
 // FP32 stencils by pairs (the FP64 path uses the per-direction forms below, in the reference's
 // order).  Mediator momentum sum_i c_i w_i 3 phi(x - c_i); the isotropic gradient
 // 3 sum_i w_i c_i phi(x + c_i) is its exact negative.

@@ -1,0 +1,82 @@
+// itlbm_snapshot.cu -- saving and restoring the state of a case (host side).
+//
+// The reference restarts an interrupted batch from step 0 (rodar_lote.py:5-7).  A snapshot holds a
+// case's description, its step count and its populations at the top of its next step, in its own
+// precision and storage form (FP64 f_R, f_B or FP32 e, d), planes of nx * ny elements without the row
+// padding.  Stepping a restored case gives the same bits the saved run would have given.
+#include "itlbm_internal.h"
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace itlbm {
+
+namespace {
+
+constexpr char MAGIC[8] = {'I', 'T', 'L', 'B', 'M', 'S', 'T', '1'};
+
+
+}  // namespace
+
+int snap_write(const char *path, const itlbm_case_desc &d, long long steps, const CaseDev &h, const void *state) {
+    SnapHeader hd{};
+    std::memcpy(hd.magic, MAGIC, 8);
+    hd.version = 1;
+    hd.desc = d;
+    hd.steps = steps;
+    const size_t elem = elem_of(h.prec), row = elem * (size_t)h.nx;
+    std::vector<unsigned char> plane(row * (size_t)h.ny);
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(ITLBM_E_IO, std::string("cannot write ") + path);
+    bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1;
+    for (int i = 0; ok && i < 2 * planes_of(h.prec); i++) {
+        const unsigned char *src = (const unsigned char *)state + (size_t)i * h.stride * elem;
+        cudaError_t e = cudaMemcpy2D(plane.data(), row, src, elem * (size_t)h.pitch, row, h.ny, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            std::fclose(f);
+            return cuda_fail(e, "snapshot copy");
+        }
+        ok = std::fwrite(plane.data(), 1, plane.size(), f) == plane.size();
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? ITLBM_OK : fail(ITLBM_E_IO, std::string("short write to ") + path);
+}
+
+int snap_read_header(const char *path, SnapHeader &hd) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(ITLBM_E_IO, std::string("cannot open ") + path);
+    const bool ok = std::fread(&hd, sizeof hd, 1, f) == 1;
+    std::fclose(f);
+    if (!ok || std::memcmp(hd.magic, MAGIC, 8) != 0 || hd.version != 1)
+        return fail(ITLBM_E_PARSE, std::string("not a case snapshot: ") + path);
+    const itlbm_case_desc &d = hd.desc;
+    if (d.nx < 1 || d.ny < 1 || (long long)d.nx * d.ny > (1LL << 30) || hd.steps < 0 ||
+        !prec_valid(d.precision))
+        return fail(ITLBM_E_PARSE, std::string("corrupt case snapshot: ") + path);
+    return ITLBM_OK;
+}
+
+int snap_read_state(const char *path, const CaseDev &h, void *state) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(ITLBM_E_IO, std::string("cannot open ") + path);
+    const size_t elem = elem_of(h.prec), row = elem * (size_t)h.nx;
+    std::vector<unsigned char> plane(row * (size_t)h.ny);
+    bool ok = std::fseek(f, (long)sizeof(SnapHeader), SEEK_SET) == 0;
+    for (int i = 0; ok && i < 2 * planes_of(h.prec); i++) {
+        ok = std::fread(plane.data(), 1, plane.size(), f) == plane.size();
+        if (!ok) break;
+        unsigned char *dst = (unsigned char *)state + (size_t)i * h.stride * elem;
+        cudaError_t e = cudaMemcpy2D(dst, elem * (size_t)h.pitch, plane.data(), row, row, h.ny, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            std::fclose(f);
+            return cuda_fail(e, "snapshot copy");
+        }
+    }
+    std::fclose(f);
+    if (!ok) return fail(ITLBM_E_PARSE, std::string("truncated case snapshot: ") + path);
+    cudaError_t e = cudaDeviceSynchronize();  // the pageable copies have landed before any stream uses them
+    return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "snapshot copy");
+}
+
+}  // namespace itlbm

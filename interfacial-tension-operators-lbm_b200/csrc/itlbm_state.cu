@@ -27,14 +27,34 @@ __device__ void store_state(const CaseDev &c, int buf, long long off, const doub
             d[(long long)i * c.stride + off] = fR[i];
             d[(long long)(NV + i) * c.stride + off] = fB[i];
         }
-    } else {
+    } else if (c.prec == ITLBM_PREC_F32) {
         float *d = (float *)c.buf[buf];
         for (int i = 0; i < NV; i++) {
             const double wr = wgt<double>(i) * c.rho0;
             d[(long long)i * c.stride + off] = (float)((fR[i] + fB[i]) - wr);
             d[(long long)(NV + i) * c.stride + off] = (float)(fR[i] - fB[i]);
         }
+    } else {  // fold: class sums of the members (FP64), then shifted and rounded
+        float *d = (float *)c.buf[buf];
+        double F[NK] = {}, Dk[NK] = {};
+        for (int i = 0; i < NV; i++) {
+            F[fold_class(i)] += fR[i] + fB[i];
+            Dk[fold_class(i)] += fR[i] - fB[i];
+        }
+        for (int K = 0; K < NK; K++) {
+            d[(long long)K * c.stride + off] = (float)(F[K] - wk<double>(K) * c.rho0);
+            d[(long long)(NK + K) * c.stride + off] = (float)Dk[K];
+        }
     }
+}
+
+// The 19 populations of a node of the fold: each class split among its members by weight (exact
+// for the class sums and every moment; a member's own share is that of the split).
+__device__ __forceinline__ void unfold_split(double E, double D, int K, int i, double rho0, double &fR, double &fB) {
+    const double share = wgt<double>(i) / wk<double>(K);
+    const double f = (wk<double>(K) * rho0 + E) * share, d = D * share;
+    fR = 0.5 * (f + d);
+    fB = 0.5 * (f - d);
 }
 
 // dist_eq (LBM_functions.cpp:890-945) of one colour
@@ -95,8 +115,22 @@ __global__ void k_export(const CaseDev *__restrict__ cp, int cur, int which, dou
                 xs = wrapi(x + cx(i), c.nx);
                 ys = wrapi(y + cy(i), c.ny);
             }
-            const long long off = (long long)ys * c.pitch + xs;
             double r, b;
+            if (c.prec == ITLBM_PREC_F32_FOLD) {
+                const int K = fold_class(i);
+                if (which) {  // the class was pushed to x + e_K
+                    xs = wrapi(x + kx(K), c.nx);
+                    ys = wrapi(y + ky(K), c.ny);
+                }
+                const long long off = (long long)ys * c.pitch + xs;
+                const float *d = (const float *)c.buf[cur];
+                unfold_split(d[(long long)K * c.stride + off], d[(long long)(NK + K) * c.stride + off], K, i,
+                             c.rho0, r, b);
+                oR[t * NV + i] = r;
+                oB[t * NV + i] = b;
+                continue;
+            }
+            const long long off = (long long)ys * c.pitch + xs;
             if (c.prec == ITLBM_PREC_F64) {
                 const double *d = (const double *)c.buf[cur];
                 r = d[(long long)i * c.stride + off];

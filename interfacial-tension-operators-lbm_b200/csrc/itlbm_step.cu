@@ -121,9 +121,11 @@ __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
 //   phase A2 rho^N of the ring from the sums;
 //   phase B  F1 / F2: gradient and normal or stress on the ring-1 region;
 //   phase C  mediator gradient, force, collision, recolouring, push to x + c_i.
-template <class S>
+// FOLD (FP32 only): the nine in-plane classes per colour instead of the 19 populations.
+template <class S, bool FOLD = false>
 __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int aux_k,
                                           SmemT<S> &sm) {
+    constexpr int NP = FOLD ? NK : NV;  // storage planes per colour
     const int tid = threadIdx.x;
     const int lx = tid % TX, ly = tid / TX;
     const int nx = c.nx, ny = c.ny, pitch = c.pitch;
@@ -139,32 +141,32 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     // ---- phase A ----------------------------------------------------------------------------
     const int x = x0 + lx, y = y0 + ly;
     const bool valid = (x < xe) && (y < ye);
-    S f[NV], sa = S(0), sb = S(0);
+    S f[NP], sa = S(0), sb = S(0);
     double sbd = 0.0;
     if (x < xe + H && y < ye + H) {
         const int xw = valid ? x : wrapi(x, nx), yw = valid ? y : wrapi(y, ny);
         const long long off = (long long)yw * pitch + xw;
-        S a[NV], b[NV];
+        S a[NP], b[NP];
 #pragma unroll
-        for (int i = 0; i < NV; i++) a[i] = ldg<LD_OWN>(src + (long long)i * stride + off);
+        for (int i = 0; i < NP; i++) a[i] = ldg<LD_OWN>(src + (long long)i * stride + off);
 #pragma unroll
-        for (int i = 0; i < NV; i++) b[i] = ldg<LD_OWN>(src + (long long)(NV + i) * stride + off);
+        for (int i = 0; i < NP; i++) b[i] = ldg<LD_OWN>(src + (long long)(NP + i) * stride + off);
 #pragma unroll
-        for (int i = 0; i < NV; i++) sa = sa + a[i];
+        for (int i = 0; i < NP; i++) sa = sa + a[i];
 #pragma unroll
-        for (int i = 0; i < NV; i++) sb = sb + b[i];
+        for (int i = 0; i < NP; i++) sb = sb + b[i];
         if constexpr (std::is_same<S, float>::value) {
             // FP32: rho^N from the FP32 sums (as for the halo nodes); the colour difference is also
             // summed in FP64 for the rest population's complement (see the split below)
 #pragma unroll
-            for (int i = 0; i < NV; i++) sbd += (double)b[i];
+            for (int i = 0; i < NP; i++) sbd += (double)b[i];
         }
         if constexpr (std::is_same<S, double>::value) {
 #pragma unroll
-            for (int i = 0; i < NV; i++) f[i] = a[i] + b[i];
+            for (int i = 0; i < NP; i++) f[i] = a[i] + b[i];
         } else {
 #pragma unroll
-            for (int i = 0; i < NV; i++) f[i] = a[i];
+            for (int i = 0; i < NP; i++) f[i] = a[i];
         }
         sm.phi[ly + HMAX][lx + HMAX] = phase_of(sa, sb, c);
     }
@@ -176,13 +178,13 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
         if (gx < xe + H && gy < ye + H) {
             const long long off = (long long)wrapi(gy, ny) * pitch + wrapi(gx, nx);
-            const S *p = src + (long long)(colour * NV) * stride + off;
-            S v[NV];
+            const S *p = src + (long long)(colour * NP) * stride + off;
+            S v[NP];
 #pragma unroll
-            for (int i = 0; i < NV; i++) v[i] = ldg<LD_RING>(p + (long long)i * stride);
+            for (int i = 0; i < NP; i++) v[i] = ldg<LD_RING>(p + (long long)i * stride);
             S acc = S(0);
 #pragma unroll
-            for (int i = 0; i < NV; i++) acc = acc + v[i];
+            for (int i = 0; i < NP; i++) acc = acc + v[i];
             sm.rsum[colour][r] = acc;
         }
     }
@@ -203,7 +205,12 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             const int gx = x0 - 1 + qx, gy = y0 - 1 + qy;
             if (gx < xe + 1 && gy < ye + 1) {
                 S g0, g1, g2;
-                if constexpr (std::is_same<S, float>::value)
+                if constexpr (FOLD) {
+                    mediator_grad_fold([&](int dx, int dy) { return sm.phi[qy + 1 + dy][qx + 1 + dx]; }, g0, g1);
+                    g0 = -g0;  // the isotropic gradient
+                    g1 = -g1;
+                    g2 = 0.f;
+                } else if constexpr (std::is_same<S, float>::value)
                     iso_grad_f32([&](int dx, int dy) { return sm.phi[qy + 1 + dy][qx + 1 + dx]; }, g0, g1, g2);
                 else
                     iso_grad(sm.phi, qx + 1, qy + 1, g0, g1, g2);
@@ -222,7 +229,10 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         const int px = lx + HMAX, py = ly + HMAX;
         S gmx, gmy, gmz;
         auto phi_at = [&](int dx, int dy) { return sm.phi[py + dy][px + dx]; };
-        if constexpr (std::is_same<S, float>::value) mediator_grad_f32(phi_at, gmx, gmy, gmz);
+        if constexpr (FOLD) {
+            mediator_grad_fold(phi_at, gmx, gmy);
+            gmz = S(0);
+        } else if constexpr (std::is_same<S, float>::value) mediator_grad_f32(phi_at, gmx, gmy, gmz);
         else mediator_grad(sm.phi, px, py, gmx, gmy, gmz);
         S Fx = S(0), Fy = S(0), Fz = S(0);
         const bool force = tipo >= ITLBM_OP_F1;
@@ -241,7 +251,8 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                 g0 = -gmx;  // the isotropic gradient is the exact negative of the mediator momentum
                 g1 = -gmy;
                 g2 = -gmz;
-                mu = chem_pot_f32(phi_at, (float)c.kf, (float)c.bf);
+                if constexpr (FOLD) mu = chem_pot_fold(phi_at, (float)c.kf, (float)c.bf);
+                else mu = chem_pot_f32(phi_at, (float)c.kf, (float)c.bf);
             } else {
                 iso_grad(sm.phi, px, py, g0, g1, g2);
                 mu = chem_pot(sm.phi, px, py, (S)c.kf, (S)c.bf);
@@ -252,13 +263,38 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         }
         const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
         const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
-        auto dst_off = [&](int i) {
-            const int xd = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
-            const int yd = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
+        auto dst_off = [&](int i) {  // D3Q19 direction i, or class i of the fold
+            const int ex = FOLD ? kx(i) : cx(i), ey = FOLD ? ky(i) : cy(i);
+            const int xd = ex == 0 ? x : (ex > 0 ? xp : xm);
+            const int yd = ey == 0 ? y : (ey > 0 ? yp : ym);
             return (long long)yd * pitch + xd;
         };
         bool skip;
-        if constexpr (std::is_same<S, double>::value) {
+        if constexpr (FOLD) {
+            RecolourFold rc;
+            if (force) collide_fold<true>(f, sa, sb, gmx, gmy, Fx, Fy, c, rc);
+            else collide_fold<false>(f, sa, sb, gmx, gmy, Fx, Fy, c, rc);
+            skip = rc.skip;
+            if (!skip) {
+                const float rho0 = (float)c.rho0;
+                double dsum = 0.0;
+                sfor<0, 4>([&](auto M) {
+                    constexpr int K = 2 * decltype(M)::value + 1;
+                    float dK, dJ;
+                    split_fold_pair<K>(rc, f[K], f[K + 1], rho0, dK, dJ);
+                    dsum += (double)dK;
+                    dsum += (double)dJ;
+                    const long long oK = dst_off(K), oJ = dst_off(K + 1);
+                    stg(&dst[(long long)K * stride + oK], f[K]);
+                    stg(&dst[(long long)(NK + K) * stride + oK], dK);
+                    stg(&dst[(long long)(K + 1) * stride + oJ], f[K + 1]);
+                    stg(&dst[(long long)(NK + K + 1) * stride + oJ], dJ);
+                });
+                const long long o0 = dst_off(0);
+                stg(&dst[o0], f[0]);
+                stg(&dst[(long long)NK * stride + o0], (float)(sbd - dsum));
+            }
+        } else if constexpr (std::is_same<S, double>::value) {
             Recolour64 rc;
             if (force) collide_f64<true>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
             else collide_f64<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
@@ -304,11 +340,11 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         }
         if (skip) {  // rho <= 1e-30: the site is streamed unchanged (Operadores_tensao.cpp:347)
             const long long off = (long long)y * pitch + x;
-            sfor<0, NV>([&](auto I) {
+            sfor<0, NP>([&](auto I) {
                 constexpr int i = decltype(I)::value;
                 const long long o = dst_off(i);
                 dst[(long long)i * stride + o] = src[(long long)i * stride + off];
-                dst[(long long)(NV + i) * stride + o] = src[(long long)(NV + i) * stride + off];
+                dst[(long long)(NP + i) * stride + o] = src[(long long)(NP + i) * stride + off];
             });
         }
 
@@ -338,7 +374,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #define ITLBM_STEP_MIN_BLOCKS (ITLBM_F32_BLOCKS * 256 / STEP_THREADS)
 #endif
 
-template <class S>
+template <class S, bool FOLD = false>
 __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(const CaseDev *__restrict__ cases,
                                                        const TileRef *__restrict__ tiles,
                                                        int ntiles, const int *__restrict__ ntiles_dev,
@@ -349,7 +385,7 @@ __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(co
         const TileRef tr = tiles[t];
         const CaseDev &c = cases[tr.case_id];
         if (k >= c.chunk_len) continue;
-        step_tile<S>(c, tr.tile, k, aux_k, sm);
+        step_tile<S, FOLD>(c, tr.tile, k, aux_k, sm);
     }
 }
 
@@ -380,6 +416,12 @@ int step_occupancy_f32() {
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<float>, STEP_THREADS, 0);
     return n;
+}
+cudaError_t launch_step_fold(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
+                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s) {
+    if (grid <= 0) return cudaSuccess;
+    k_step<float, true><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
+    return cudaGetLastError();
 }
 #endif
 

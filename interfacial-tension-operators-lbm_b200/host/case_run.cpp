@@ -2,12 +2,109 @@
 #include "case_run.h"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <iostream>
+#include <sstream>
 
 namespace itlbm_host {
 
 namespace {
 const double U_LIMITE = 0.4;  // Imm_OPS.cpp:45, Imm_INCL.cpp:43
+}
+
+namespace {
+
+// Rows of a diagnostic text file with a step number (first column) up to `upto`, header lines kept.
+std::string rows_upto(const std::string &path, int upto) {
+    std::ifstream in(path);
+    std::string out, ln;
+    while (std::getline(in, ln)) {
+        if (!ln.empty() && ln[0] != '#') {
+            std::istringstream ss(ln);
+            double st;
+            if (!(ss >> st) || st > upto) continue;
+        }
+        out += ln + "\n";
+    }
+    return out;
+}
+
+bool reopen(std::ofstream &f, const std::string &path, int upto) {
+    const std::string kept = rows_upto(path, upto);
+    f.open(path);
+    if (!f) return false;
+    f << kept;
+    f.flush();
+    return true;
+}
+
+template <size_t N>
+bool write_hist(const std::string &path, const std::vector<std::array<double, N>> &h) {
+    std::ofstream f(path + ".tmp");
+    if (!f) return false;
+    char b[40];
+    for (const auto &r : h) {
+        for (size_t k = 0; k < N; k++) {
+            std::snprintf(b, sizeof b, "%a", r[k]);  // exact
+            f << (k ? " " : "") << b;
+        }
+        f << "\n";
+    }
+    f.close();
+    return std::rename((path + ".tmp").c_str(), path.c_str()) == 0;
+}
+
+template <size_t N>
+bool read_hist(const std::string &path, int upto, std::vector<std::array<double, N>> &h) {
+    std::ifstream f(path);
+    if (!f) return false;
+    h.clear();
+    for (std::string ln; std::getline(f, ln);) {
+        std::istringstream ss(ln);
+        std::array<double, N> r{};
+        std::string w;
+        size_t k = 0;
+        for (; k < N && ss >> w; k++) r[k] = std::strtod(w.c_str(), nullptr);
+        if (k != N) return false;
+        if (r[0] <= upto) h.push_back(r);
+    }
+    return true;
+}
+
+}  // namespace
+
+void DropRun::account(const std::array<double, 10> &r) {
+    const int step = (int)r[0];
+    neg_total_max = std::max(neg_total_max, (long long)r[7]);
+    neg_cor_max = std::max(neg_cor_max, (long long)r[8]);
+    min_f_global = std::min(min_f_global, r[9]);
+    if (step >= n_steps / 2) {
+        s_sigma += r[1];
+        s_umax += r[2];
+        s_urms += r[3];
+        s_a4 += r[4];
+        s_a8 += r[5];
+        s_K += r[6];
+        n_med++;
+    }
+}
+
+bool DropRun::save_hist(const std::string &path) const { return write_hist(path, hist); }
+
+bool DropRun::resume(const std::string &dir, double tau, double v0_, int n_steps_, int upto,
+                     const std::string &hist_file) {
+    nu = (1. / 3.) * (tau - 0.5);
+    v0 = v0_;
+    n_steps = n_steps_;
+    if (!read_hist(hist_file, upto, hist)) return false;
+    for (const auto &r : hist) account(r);
+    if (!(reopen(lap, join(dir, "laplace.dat"), upto) && reopen(iso, join(dir, "iso.dat"), upto) &&
+          reopen(gi, join(dir, "galilean.dat"), upto)))
+        return false;
+    lap << std::setprecision(10);  // as open() sets them
+    iso << std::setprecision(10);
+    return true;
 }
 
 bool DropRun::open(const std::string &dir, double tau, double v0_, int n_steps_) {
@@ -44,18 +141,9 @@ bool DropRun::on_diag(int step, const itlbm_drop_diag &dg, std::ostream *log) {
         iso << step << " " << dg.R0 << " " << dg.a2 << " " << dg.a4 << " " << dg.a8 << " " << dg.rmin << " "
             << dg.rmax << "\n";
         iso.flush();
-        neg_total_max = std::max(neg_total_max, dg.negative_total);
-        neg_cor_max = std::max(neg_cor_max, dg.negative_color);
-        min_f_global = std::min(min_f_global, dg.min_f);
-        if (step >= n_steps / 2) {
-            s_sigma += dg.sigma;
-            s_umax += dg.u_max;
-            s_urms += dg.u_rms;
-            s_a4 += dg.a4;
-            s_a8 += dg.a8;
-            s_K += dg.K_perfil;
-            n_med++;
-        }
+        hist.push_back({(double)step, dg.sigma, dg.u_max, dg.u_rms, dg.a4, dg.a8, dg.K_perfil,
+                        (double)dg.negative_total, (double)dg.negative_color, dg.min_f});
+        account(hist.back());
         if (log)
             *log << "\rstep = " << step << "   R = " << dg.raio << "   sigma = " << dg.sigma
                  << "   |u|max = " << dg.u_max << "   a4 = " << dg.a4 << "   neg = " << dg.negative_total
@@ -101,6 +189,39 @@ bool StripRun::open(const std::string &dir, int n_steps_, int p_, int q_) {
     return true;
 }
 
+void StripRun::account(const std::array<double, 12> &r) {
+    const int step = (int)r[0];
+    if (step == 0) d0_ini = r[8];
+    d0_fim = r[8];
+    neg_t = std::max(neg_t, (long long)r[9]);
+    neg_c = std::max(neg_c, (long long)r[10]);
+    min_f = std::min(min_f, r[11]);
+    if (step >= n_steps / 2) {
+        s_sig += r[1];
+        s_um += r[2];
+        s_un += r[3];
+        s_ut += r[4];
+        s_K += r[5];
+        s_res += r[6];
+        s_ig += r[7];
+        n_med++;
+    }
+}
+
+bool StripRun::save_hist(const std::string &path) const { return write_hist(path, hist); }
+
+bool StripRun::resume(const std::string &dir, int n_steps_, int p_, int q_, int upto,
+                      const std::string &hist_file) {
+    n_steps = n_steps_;
+    p = p_;
+    q = q_;
+    if (!read_hist(hist_file, upto, hist)) return false;
+    for (const auto &r : hist) account(r);
+    if (!reopen(inc, join(dir, "inclinada.dat"), upto)) return false;
+    inc << std::setprecision(10);
+    return true;
+}
+
 bool StripRun::on_diag(int step, const itlbm_strip_diag &r, std::ostream *log) {
     const bool ok = r.ok != 0;
     inc << step << " " << r.sigma_pop << " " << r.int_grad << " " << r.K << " "
@@ -109,21 +230,9 @@ bool StripRun::on_diag(int step, const itlbm_strip_diag &r, std::ostream *log) {
         << " " << r.qy << " " << r.SFx << " " << r.SFy << " " << r.min_f << " " << r.neg_total << " "
         << r.neg_cor << "\n";
     inc.flush();
-    if (step == 0) d0_ini = r.d0;
-    d0_fim = r.d0;
-    neg_t = std::max(neg_t, r.neg_total);
-    neg_c = std::max(neg_c, r.neg_cor);
-    min_f = std::min(min_f, r.min_f);
-    if (step >= n_steps / 2) {
-        s_sig += r.sigma_pop;
-        s_um += r.u_max;
-        s_un += r.un_max;
-        s_ut += r.ut_max;
-        s_K += r.K;
-        s_res += r.res;
-        s_ig += r.int_grad;
-        n_med++;
-    }
+    hist.push_back({(double)step, r.sigma_pop, r.u_max, r.un_max, r.ut_max, r.K, r.res, r.int_grad, r.d0,
+                    (double)r.neg_total, (double)r.neg_cor, r.min_f});
+    account(hist.back());
     if (log)
         *log << "\rstep = " << step << "   sigma_pop = " << r.sigma_pop << "   K = " << r.K
              << "   |u|max = " << r.u_max << "   neg = " << r.neg_total << "        " << std::endl;

@@ -4,10 +4,12 @@
 //   StripRun  Imm_INCL.cpp:338-350, :404-434, :446-460
 #pragma once
 
+#include <array>
 #include <cmath>
 #include <fstream>
 #include <iomanip>
 #include <string>
+#include <vector>
 
 #include "case_io.h"
 
@@ -24,9 +26,20 @@ struct DropRun {
     std::string estado = "estavel";
     int passo_falha = -1;
 
+    // per diagnostic row, at full precision: step, sigma, u_max, u_rms, a4, a8, K_perfil,
+    // negative_total, negative_color, min_f (what the means and maxima of resumo.dat are made of)
+    std::vector<std::array<double, 10>> hist;
+
     bool open(const std::string &dir, double tau, double v0_, int n_steps_);
     // One diagnostic step; returns true when the stop rule fires (Imm_OPS.cpp:346-352).
     bool on_diag(int step, const itlbm_drop_diag &dg, std::ostream *log);
+    // Resuming from a snapshot: keep the rows of laplace.dat, iso.dat and galilean.dat up to step
+    // `upto`, append after them, and rebuild the accounting from the saved history (`hist_file`),
+    // replayed in order so that the means come out as they would have without the interruption.
+    bool resume(const std::string &dir, double tau, double v0_, int n_steps_, int upto,
+                const std::string &hist_file);
+    bool save_hist(const std::string &path) const;
+    void account(const std::array<double, 10> &r);
     void write_resumo(const std::string &dir, const itlbm_operador &op, double tau, double beta,
                       double A_in, int nx, double raio_ini, double sigma_nominal, int steps,
                       double mlups) const;
@@ -42,8 +55,15 @@ struct StripRun {
     std::string estado = "estavel";
     int passo_falha = -1;
 
+    // per diagnostic row: step, sigma_pop, u_max, un_max, ut_max, K, res, int_grad, d0, neg_total,
+    // neg_cor, min_f
+    std::vector<std::array<double, 12>> hist;
+
     bool open(const std::string &dir, int n_steps_, int p_, int q_);
     bool on_diag(int step, const itlbm_strip_diag &r, std::ostream *log);
+    bool resume(const std::string &dir, int n_steps_, int p_, int q_, int upto, const std::string &hist_file);
+    bool save_hist(const std::string &path) const;
+    void account(const std::array<double, 12> &r);
     void write_resumo(const std::string &dir, const itlbm_operador &op, double tau, double beta,
                       double A_in, int N, double theta, double sigma_nominal, int steps,
                       double mlups) const;

@@ -1,7 +1,7 @@
 // itlbm_serve -- continuous batching of case folders on one GPU.
 //
 //   itlbm_serve <spool-dir> [--budget-gb G] [--chunk K] [--fp64] [--idle-exit S] [--max-cases M]
-//               [--summary-root DIR]
+//               [--summary-root DIR] [--snapshots]
 //
 // The reference runs one process per case folder (rodar_lote.py:231-243).  This server keeps one
 // batch (itlbm_batch_*) on the device and admits case folders as they arrive:
@@ -18,7 +18,11 @@
 //     <name>.done with its time-to-result;
 //   * <spool>/serve_stats.json keeps the count, p50 / p99 time-to-result and the aggregate MLUPS;
 //   * <spool>/resumo_gota.csv and resumo_incl.csv get each retired case's row of the batch tables of
-//     analisar_lote.py (folders named relative to --summary-root), so they need no post-pass.
+//     analisar_lote.py (folders named relative to --summary-root), so they need no post-pass;
+//   * with --snapshots, each case's state is saved in its folder (estado_itlbm.bin, with the
+//     diagnostic history in estado_itlbm.run) at every diagnostic; a request for a folder holding a
+//     snapshot of the same case short of its step count resumes from it instead of step 0 (the
+//     reference restarts from step 0, rodar_lote.py:5-7), with the same results.
 // The client bin/itlbm_submit turns this into a drop-in for the Imm_OPS binary of rodar_lote.py.
 // The final VTK fields and perfil.dat are written only by itlbm_ops / itlbm_incl.
 #include <algorithm>
@@ -52,6 +56,7 @@ struct Job {
     std::string name, dir;
     itlbm_case_desc desc{};
     bool strip = false;
+    long long resume_steps = 0;  // > 0: restart from the folder's snapshot, taken after this many steps
     int n_steps = 0, nx = 0;
     double raio_ini = 0, sigma_nominal = 0, theta = 0, beta = 0, A = 0, tau = 0;
     double t_submit = 0;
@@ -84,8 +89,20 @@ void write_text(const std::string &path, const std::string &text) {
     std::rename((path + ".tmp").c_str(), path.c_str());
 }
 
-// Reads and validates a case folder like Imm_OPS.cpp:65-135 / Imm_INCL.cpp:192-266.
-bool prepare(Job &j, bool fp64, std::string &err) {
+const char *SNAP_FILE = "estado_itlbm.bin";  // the case's state after its last snapshot
+const char *HIST_FILE = "estado_itlbm.run";  // its diagnostic history, for the resumo.dat means
+
+bool same_desc(const itlbm_case_desc &a, const itlbm_case_desc &b) {
+    return a.nx == b.nx && a.ny == b.ny && a.op.tipo == b.op.tipo && a.op.chi == b.op.chi && a.op.xi == b.op.xi &&
+           a.tau == b.tau && a.beta == b.beta && a.A_fact == b.A_fact && a.rho_R == b.rho_R && a.rho_B == b.rho_B &&
+           a.geometry == b.geometry && a.radius == b.radius && a.k_profile == b.k_profile && a.v0 == b.v0 &&
+           a.p == b.p && a.q == b.q && a.precision == b.precision;
+}
+
+// Reads and validates a case folder like Imm_OPS.cpp:65-135 / Imm_INCL.cpp:192-266.  With
+// `snapshots`, a folder holding a snapshot of the same case that is short of its step count resumes
+// from it (its output files keep their rows up to the snapshot).
+bool prepare(Job &j, bool fp64, bool snapshots, std::string &err) {
     std::ostringstream log;
     DataIn din;
     if (!read_data(j.dir, din, log)) {
@@ -155,15 +172,29 @@ bool prepare(Job &j, bool fp64, std::string &err) {
         err = "steps < 1";
         return false;
     }
+    j.resume_steps = 0;
+    if (snapshots) {
+        itlbm_case_desc sd;
+        long long steps = 0;
+        if (stat(join(j.dir, HIST_FILE).c_str(), &st) == 0 &&
+            itlbm_snapshot_info(join(j.dir, SNAP_FILE).c_str(), &sd, &steps) == ITLBM_OK && same_desc(sd, d) &&
+            steps > 0 && steps < j.n_steps)
+            j.resume_steps = steps;
+    }
+    const int upto = (int)j.resume_steps - 1;  // the last diagnostic step before the snapshot
     if (j.strip) {
         j.stp.reset(new StripRun());
-        if (!j.stp->open(j.dir, j.n_steps, p, q)) {
+        const bool ok = j.resume_steps ? j.stp->resume(j.dir, j.n_steps, p, q, upto, join(j.dir, HIST_FILE))
+                                       : j.stp->open(j.dir, j.n_steps, p, q);
+        if (!ok) {
             err = "cannot write inclinada.dat";
             return false;
         }
     } else {
         j.drop.reset(new DropRun());
-        if (!j.drop->open(j.dir, j.tau, v0, j.n_steps)) {
+        const bool ok = j.resume_steps ? j.drop->resume(j.dir, j.tau, v0, j.n_steps, upto, join(j.dir, HIST_FILE))
+                                       : j.drop->open(j.dir, j.tau, v0, j.n_steps);
+        if (!ok) {
             err = "cannot write the output files";
             return false;
         }
@@ -185,7 +216,7 @@ double percentile(std::vector<double> v, double p) {
 int main(int argc, char **argv) {
     if (argc < 2) {
         std::cerr << "usage: itlbm_serve <spool-dir> [--budget-gb G] [--chunk K] [--fp64] [--idle-exit S] "
-                     "[--max-cases M] [--summary-root DIR]\n";
+                     "[--max-cases M] [--summary-root DIR] [--snapshots]\n";
         return 1;
     }
     const std::string spool = argv[1];
@@ -193,6 +224,7 @@ int main(int argc, char **argv) {
     int chunk = 500, max_cases = 0;
     bool fp64_default = false;
     std::string summary_root;  // case folders are named relative to it in the batch tables
+    bool snapshots = false;    // snapshot every case at each diagnostic and resume from snapshots
     for (int a = 2; a < argc; a++) {
         const std::string k = argv[a];
         if (k == "--budget-gb" && a + 1 < argc) budget_gb = std::atof(argv[++a]);
@@ -201,6 +233,7 @@ int main(int argc, char **argv) {
         else if (k == "--max-cases" && a + 1 < argc) max_cases = std::atoi(argv[++a]);
         else if (k == "--fp64") fp64_default = true;
         else if (k == "--summary-root" && a + 1 < argc) summary_root = argv[++a];
+        else if (k == "--snapshots") snapshots = true;
     }
     itlbm_batch_config cfg{};
     cfg.hbm_budget = (size_t)(budget_gb * 1e9);
@@ -233,7 +266,7 @@ int main(int argc, char **argv) {
             j.dir = dir;
             std::string err;
             const bool fp64 = prec == "fp64" || (prec != "fp32" && fp64_default);
-            if (!prepare(j, fp64, err)) {
+            if (!prepare(j, fp64, snapshots, err)) {
                 write_text(join(spool, name + ".err"), err + "\n");
                 std::remove(run.c_str());
                 failed_inputs++;
@@ -241,7 +274,10 @@ int main(int argc, char **argv) {
             }
             j.t_submit = now_s();
             const long long tag = next_tag++;
-            if (itlbm_batch_submit(b, &j.desc, j.n_steps, tag) != ITLBM_OK) {
+            const int sub = j.resume_steps
+                                ? itlbm_batch_submit_saved(b, join(j.dir, SNAP_FILE).c_str(), j.n_steps, tag)
+                                : itlbm_batch_submit(b, &j.desc, j.n_steps, tag);
+            if (sub != ITLBM_OK) {
                 write_text(join(spool, name + ".err"), std::string("admission: ") + itlbm_last_error() + "\n");
                 std::remove(run.c_str());
                 failed_inputs++;
@@ -272,6 +308,18 @@ int main(int argc, char **argv) {
                 if (e.kind == ITLBM_EV_DIAG) {
                     if (j.drop) j.drop->on_diag(e.step, e.drop, nullptr);
                     else j.stp->on_diag(e.step, e.strip, nullptr);
+                    if (snapshots) {
+                        // the history first, then the state (a case that retired in this round has no
+                        // state left to save, and needs none)
+                        const bool hist_ok = j.drop ? j.drop->save_hist(join(j.dir, HIST_FILE))
+                                                    : j.stp->save_hist(join(j.dir, HIST_FILE));
+                        const std::string snap = join(j.dir, SNAP_FILE);
+                        const int rs = hist_ok ? itlbm_batch_save(b, e.tag, (snap + ".tmp").c_str()) : ITLBM_E_IO;
+                        if (rs == ITLBM_OK) std::rename((snap + ".tmp").c_str(), snap.c_str());
+                        else if (!(j.n_steps - 1 == e.step))  // the last step has no state left to save
+                            std::cerr << "itlbm_serve: no snapshot of " << j.dir << " at step " << e.step << ": "
+                                      << (hist_ok ? itlbm_last_error() : "history not written") << std::endl;
+                    }
                     continue;
                 }
                 const double t = now_s(), latency = t - j.t_submit;

@@ -1,0 +1,117 @@
+"""The FP32 fold (ITLBM_PREC_F32_FOLD): the nine in-plane classes of D3Q19 per colour.  For the
+one-node slab the class sums of the 19 populations evolve exactly as the folded lattice, so the fold
+must follow the FP64 path (bit-identical to the reference) as closely as the 19-population FP32
+storage does: class sums after 300 steps within FP32 rounding, and the observables of the accuracy
+bar of the FP32 storage after 2000 steps (Laplace jump 0.5 %, peak spurious velocity 5 %, radius
+2e-4, colour masses 2e-7), for every operator and for the inclined strip."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+OPS = [("P1", 1, 0.5, 1.569988, 0.225), ("P3 0.5", 3, 0.5, 1.569988, 0.225), ("P3 2", 3, 2.0, 1.569988, 0.225),
+       ("F1", 11, 0.5, 1.569988, 0.1), ("F2", 12, 0.5, 1.569988, 0.1), ("F3", 13, 0.5, 1.569988, 0.1)]
+CLASS = [0, 1, 2, 3, 4, 0, 0, 5, 6, 7, 8, 1, 2, 1, 2, 4, 3, 4, 3]
+
+
+def case(itlbm, nx, tipo, chi, xi, A, prec, geometry=0, p=1, q=0, v0=0.0, tau=0.8, radius=16.0):
+    op = itlbm.make_op(tipo, chi, xi)
+    d = itlbm.desc(nx, nx, op, tau=tau, A_fact=A, radius=radius, k_profile=2.0 * math.log(9.0) / 3.45,
+                   v0=v0, geometry=geometry, p=p, q=q, precision=prec)
+    return itlbm.Case(d)
+
+
+def fold(pops):
+    fR, fB = pops
+    n = fR.size // 19
+    out = np.zeros((2, n, 9))
+    for i, K in enumerate(CLASS):
+        out[0, :, K] += fR.reshape(n, 19)[:, i]
+        out[1, :, K] += fB.reshape(n, 19)[:, i]
+    return out
+
+
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=[o[0] for o in OPS])
+def test_fold_class_sums_follow_fp64(gpu, name, tipo, chi, xi, A):
+    c64 = case(gpu, 64, tipo, chi, xi, A, gpu.PREC_F64, v0=0.03)
+    c32 = case(gpu, 64, tipo, chi, xi, A, gpu.PREC_F32, v0=0.03)
+    cf = case(gpu, 64, tipo, chi, xi, A, gpu.PREC_F32_FOLD, v0=0.03)
+    try:
+        assert np.allclose(fold(c64.read_pops(0)), fold(cf.read_pops(0)), rtol=0, atol=1e-7)
+        for c in (c64, c32, cf):
+            c.step(300)
+        ref = fold(c64.read_pops(0))
+        err_fold = np.abs(fold(cf.read_pops(0)) - ref).max()
+        err_f32 = np.abs(fold(c32.read_pops(0)) - ref).max()
+        # the fold carries no more rounding than the 19-population FP32 storage (with some slack)
+        assert err_fold <= max(4 * err_f32, 2e-6), (err_fold, err_f32)
+    finally:
+        for c in (c64, c32, cf):
+            c.close()
+
+
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=[o[0] for o in OPS])
+def test_fold_tracks_fp64(gpu, name, tipo, chi, xi, A):
+    c64 = case(gpu, 80, tipo, chi, xi, A, gpu.PREC_F64)
+    cf = case(gpu, 80, tipo, chi, xi, A, gpu.PREC_F32_FOLD)
+    try:
+        m0 = [x.sum() for x in cf.read_pops(0)]
+        for c in (c64, cf):
+            c.step(1999)
+            c.step(1, keep_aux=True)
+        d64, df = c64.diag_drop(1999), cf.diag_drop(1999)
+        m1 = [x.sum() for x in cf.read_pops(0)]
+        print(f"{name}: dp {df.delta_p / d64.delta_p - 1:+.2e}  umax {df.u_max / d64.u_max - 1:+.2e}  "
+              f"R {df.raio / d64.raio - 1:+.2e}  mass_R {m1[0] / m0[0] - 1:+.2e}")
+        assert df.ok
+        assert abs(df.delta_p - d64.delta_p) <= 5e-3 * abs(d64.delta_p)
+        assert abs(df.u_max - d64.u_max) <= 0.05 * d64.u_max
+        assert abs(df.raio - d64.raio) <= 2e-4 * d64.raio
+        assert abs(m1[0] - m0[0]) <= 2e-7 * m0[0] and abs(m1[1] - m0[1]) <= 2e-7 * m0[1]
+        f64, ff = c64.read_fields(force=True), cf.read_fields(force=True)
+        assert np.abs(ff["force"] - f64["force"]).max() <= 1e-3 * max(np.abs(f64["force"]).max(), 1e-12)
+    finally:
+        c64.close()
+        cf.close()
+
+
+def test_fold_strip_and_batch(gpu):
+    """An inclined strip in the fold tracks FP64 (the interface-normal quantities; sigma_pop needs P_zz,
+    which the fold only has as its weight split), and fold cases give the same bits in a batch as alone."""
+    c64 = case(gpu, 60, 12, 0.5, 1.569988, 0.1, gpu.PREC_F64, geometry=1, p=2, q=1)
+    cf = case(gpu, 60, 12, 0.5, 1.569988, 0.1, gpu.PREC_F32_FOLD, geometry=1, p=2, q=1)
+    try:
+        for c in (c64, cf):
+            c.step(999)
+            c.step(1, keep_aux=True)
+        s64, sf = c64.diag_strip(999), cf.diag_strip(999)
+        # the interface offset d0 is a hundredth of a node here, at the level of the rounding of
+        # either storage: compared in nodes
+        assert sf.ok and abs(sf.K - s64.K) <= 1e-3 * abs(s64.K) and abs(sf.d0 - s64.d0) <= 0.03
+        assert abs(sf.int_grad - s64.int_grad) <= 1e-4 * abs(s64.int_grad)
+    finally:
+        c64.close()
+        cf.close()
+    descs = []
+    for nx, tipo in ((64, 3), (50, 13), (72, 11)):
+        op = gpu.make_op(tipo, 0.5, 1.569988)
+        descs.append(gpu.desc(nx, nx, op, tau=0.8, A_fact=0.1, precision=gpu.PREC_F32_FOLD))
+    rows = {}
+    with gpu.Batch(chunk=100, diag_every=250) as b:
+        for k, d in enumerate(descs):
+            b.submit(d, 251, k)
+        for _ in range(20):
+            b.advance()
+            for e in b.poll():
+                if e.kind == gpu.EV_DIAG:
+                    rows[(e.tag, e.step)] = e.drop.as_dict()
+            if b.stats().active == 0:
+                break
+    for k, d in enumerate(descs):
+        with gpu.Case(d) as c:
+            c.step(251, keep_aux=True)
+            alone = c.diag_drop(250).as_dict()
+        for key in ("massa_R", "u_max", "raio", "delta_p"):
+            assert alone[key] == rows[(k, 250)][key], (k, key)

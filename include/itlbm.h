@@ -247,6 +247,11 @@ typedef struct itlbm_batch_stats {
     double    device_ms;      /* device time of the step launches (CUDA events)                  */
     size_t    hbm_used;       /* bytes of case state held                                         */
     int       replays;        /* graph replays so far                                              */
+    int       captures;       /* graph (re)captures so far: the work tables changed their grid     */
+    double    diag_ms;        /* device time of the diagnostics (CUDA events)                      */
+    double    advance_ms;     /* host wall time spent inside itlbm_batch_advance                   */
+    double    admit_ms;       /* of which admission: allocation and initial state of new cases     */
+    double    capture_ms;     /* of which graph capture and instantiation                          */
 } itlbm_batch_stats;
 
 /* No case memory is allocated until cases are admitted. */

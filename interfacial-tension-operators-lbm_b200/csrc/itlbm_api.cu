@@ -85,6 +85,10 @@ void case_layout(CaseDev &h, int nx, int ny, int prec, bool march) {
 
 int case_items(const CaseDev &h) { return h.march ? h.m_items : h.tiles; }
 
+int item_code(const CaseDev &h, int k) {
+    return h.march ? k : (int)(((unsigned)(k / h.tiles_x) << 16) | (unsigned)(k % h.tiles_x));
+}
+
 cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf) {
     h.buf[0] = mem;
     h.buf[1] = (char *)mem + per_buf;
@@ -208,7 +212,7 @@ void itlbm_case_destroy(itlbm_case *c) {
 int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
     if (!d || !out) return fail(ITLBM_E_ARG, "NULL argument");
     *out = nullptr;
-    if (d->nx < 1 || d->ny < 1 || (long long)d->nx * d->ny > (1LL << 30))
+    if (d->nx < 1 || d->ny < 1 || (long long)d->nx * d->ny > (1LL << 30) || !box_tileable(d->nx, d->ny))
         return fail(ITLBM_E_ARG, "box size out of range");
     if (!op_valid(d->op.tipo)) return fail(ITLBM_E_ARG, "unknown operator");
     if (!(d->tau > 0.0) || !std::isfinite(d->tau)) return fail(ITLBM_E_ARG, "tau must be > 0");
@@ -247,7 +251,7 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
     h.aux = nullptr;
     c->ntiles = case_items(h);
     std::vector<TileRef> tl(c->ntiles);
-    for (int t = 0; t < c->ntiles; t++) tl[t] = TileRef{0, t};
+    for (int t = 0; t < c->ntiles; t++) tl[t] = TileRef{0, item_code(h, t)};
     if ((e = cudaMalloc(&c->tiles, sizeof(TileRef) * c->ntiles)) != cudaSuccess ||
         (e = cudaMalloc(&c->dev, sizeof(CaseDev))) != cudaSuccess) {
         itlbm_case_destroy(c);

@@ -77,6 +77,13 @@ struct itlbm_batch {
     itlbm_batch_config cfg{};
     int device = 0, sms = 0;
     cudaStream_t stream = nullptr;
+    // case state comes from a stream-ordered pool that keeps up to the HBM budget reserved:
+    // admissions and retirements neither map nor unmap device memory nor synchronise the device
+    cudaMemPool_t pool = nullptr;
+    // initial profiles of the cases admitted in one round, in mapped pinned host memory that the
+    // init kernel reads directly (no device staging buffer to allocate and free per case)
+    double *stage = nullptr, *stage_dev = nullptr;
+    size_t stage_cap = 0, stage_used = 0;
     std::deque<Pending> pending;
     std::vector<Active *> slots;
     std::vector<int> free_slots;
@@ -90,6 +97,10 @@ struct itlbm_batch {
     bool march = false;  // FP32 cases run the marching kernel
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // one chain of step launches per non-empty table, each on its own stream between a fork and a
+    // join on `stream`: the tables hold different cases, so their steps need no order between them
+    cudaStream_t side[NTAB] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[NTAB] = {};
     DiagScratch diag;
     int diag_nx = 0, diag_ny = 0;
     itlbm_drop_diag *d_drop = nullptr;
@@ -100,8 +111,9 @@ struct itlbm_batch {
     std::chrono::steady_clock::time_point t0;
     size_t hbm_used = 0;
     long long node_updates = 0;
-    double device_ms = 0;
-    int replays = 0, finished = 0;
+    double device_ms = 0, diag_ms = 0, advance_ms = 0, admit_ms = 0, capture_ms = 0;
+    int replays = 0, finished = 0, captures = 0;
+    cudaEvent_t ev2 = nullptr;  // end of the diagnostics
 
     double now() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -110,6 +122,16 @@ struct itlbm_batch {
 
 namespace {
 
+// Grid of a table of n tiles: n rounded up to m x 2^e with m < 32 (at most 1/16 more CTAs, which
+// exit at once), so that admissions and retirements change the grid -- and re-capture the graph --
+// only when the table crosses a bucket.
+int grid_bucket(int n) {
+    if (n <= 32) return n;
+    int e = 0;
+    while ((n >> e) >= 32) e++;
+    return ((n + (1 << e) - 1) >> e) << e;
+}
+
 int upload_tables(itlbm_batch *b) {
     std::vector<TileRef> t[NTAB];
     for (Active *a : b->slots) {
@@ -117,7 +139,7 @@ int upload_tables(itlbm_batch *b) {
         const CaseDev &c = b->h_cases[a->slot];
         const int p = table_of(a->desc.precision);
         const int n = case_items(c);
-        for (int k = 0; k < n; k++) t[p].push_back(TileRef{a->slot, k});
+        for (int k = 0; k < n; k++) t[p].push_back(TileRef{a->slot, item_code(c, k)});
     }
     int n[NTAB];
     for (int p = 0; p < NTAB; p++) {
@@ -135,14 +157,52 @@ int upload_tables(itlbm_batch *b) {
         }
     }
     if (b->cfg.ctas_per_sm <= 0)
-        for (int p = 0; p < NTAB; p++) b->grid[p] = n[p];
+        for (int p = 0; p < NTAB; p++) b->grid[p] = grid_bucket(n[p]);
     // the graph reads the table pointers it was captured with: keep them, or re-capture
     cudaError_t e = cudaMemcpyAsync(b->d_ntiles, n, sizeof(int) * NTAB, cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "work table length");
     return cudaStreamSynchronize(b->stream) == cudaSuccess ? ITLBM_OK : cuda_fail(cudaGetLastError(), "sync");
 }
 
+// K sub-steps of every table on the batch stream: one table runs in line, several run as parallel
+// chains (fork, one chain per table on its own stream, join), in a capture or directly.
+cudaError_t enqueue_steps(itlbm_batch *b, int K) {
+    int used = 0;
+    for (int p = 0; p < NTAB; p++) used += b->grid[p] > 0;
+    cudaError_t e = cudaSuccess;
+    if (used <= 1) {
+        for (int p = 0; p < NTAB; p++)
+            for (int k = 0; k < K && b->grid[p] > 0 && e == cudaSuccess; k++)
+                e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
+                                prec_of_table(p), p == 1 && b->march, b->stream);
+        return e;
+    }
+    if ((e = cudaEventRecord(b->ev_fork, b->stream)) != cudaSuccess) return e;
+    for (int p = 0; p < NTAB; p++) {
+        if (b->grid[p] <= 0) continue;
+        if ((e = cudaStreamWaitEvent(b->side[p], b->ev_fork, 0)) != cudaSuccess) return e;
+        for (int k = 0; k < K && e == cudaSuccess; k++)
+            e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
+                            prec_of_table(p), p == 1 && b->march, b->side[p]);
+        if (e != cudaSuccess) return e;
+        if ((e = cudaEventRecord(b->ev_join[p], b->side[p])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(b->stream, b->ev_join[p], 0)) != cudaSuccess) return e;
+    }
+    return e;
+}
+
+// Adds the host wall time of its scope to a counter of the batch, in ms.
+struct ScopeTimer {
+    const itlbm_batch *b;
+    double &acc;
+    double t;
+    ScopeTimer(const itlbm_batch *b_, double &acc_) : b(b_), acc(acc_), t(b_->now()) {}
+    ~ScopeTimer() { acc += (b->now() - t) * 1e3; }
+};
+
 int capture_graph(itlbm_batch *b) {
+    ScopeTimer timer(b, b->capture_ms);
+    b->captures++;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -150,12 +210,12 @@ int capture_graph(itlbm_batch *b) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "begin capture");
-    for (int k = 0; k < b->cfg.chunk; k++) {
-        for (int p = 0; p < NTAB; p++)
-            launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
-                        p == 1 && b->march, b->stream);
-    }
+    const cudaError_t el = enqueue_steps(b, b->cfg.chunk);
     e = cudaStreamEndCapture(b->stream, &g);
+    if (el != cudaSuccess) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return cuda_fail(el, "captured step launches");
+    }
     if (e != cudaSuccess) return cuda_fail(e, "end capture");
     e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
@@ -163,8 +223,8 @@ int capture_graph(itlbm_batch *b) {
 }
 
 void retire(itlbm_batch *b, Active *a) {
-    cudaFree(a->mem);
-    if (a->aux) cudaFree(a->aux);
+    cudaFreeAsync(a->mem, b->stream);
+    if (a->aux) cudaFreeAsync(a->aux, b->stream);
     b->hbm_used -= a->bytes;
     b->slots[a->slot] = nullptr;
     b->free_slots.push_back(a->slot);
@@ -174,7 +234,28 @@ void retire(itlbm_batch *b, Active *a) {
     delete a;
 }
 
+// Room for `len` profile values in the staging buffer: wait for the round's earlier initial states
+// when it is full, grow it when one profile does not fit.
+cudaError_t stage_reserve(itlbm_batch *b, size_t len) {
+    if (b->stage_used + len <= b->stage_cap) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    if (b->stage_used > 0 && (e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return e;
+    b->stage_used = 0;
+    if (len <= b->stage_cap) return cudaSuccess;
+    if (b->stage) cudaFreeHost(b->stage);
+    b->stage = b->stage_dev = nullptr;
+    b->stage_cap = 0;
+    const size_t cap = std::max<size_t>(len, (size_t)1 << 20);
+    if ((e = cudaHostAlloc((void **)&b->stage, sizeof(double) * cap, cudaHostAllocMapped | cudaHostAllocPortable)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaHostGetDevicePointer((void **)&b->stage_dev, b->stage, 0)) != cudaSuccess) return e;
+    b->stage_cap = cap;
+    return cudaSuccess;
+}
+
 int admit(itlbm_batch *b) {
+    b->stage_used = 0;  // the previous round's initial states are complete (advance ends synchronised)
     while (!b->pending.empty() && !b->free_slots.empty()) {
         const Pending &p = b->pending.front();
         bool need_aux;
@@ -192,17 +273,18 @@ int admit(itlbm_batch *b) {
         fill_params(h, d.op, d.tau, d.A_fact, d.beta, d.rho_B > 0 ? d.rho_B : 1.0);
         const size_t elem = elem_of(d.precision);
         const size_t per_buf = (size_t)2 * planes_of(d.precision) * h.stride * elem;
-        cudaError_t e = cudaMalloc(&a->mem, 2 * per_buf);
-        if (e == cudaSuccess && need_aux) e = cudaMalloc(&a->aux, sizeof(double) * 4 * (size_t)h.stride);
+        cudaError_t e = cudaMallocFromPoolAsync(&a->mem, 2 * per_buf, b->pool, b->stream);
+        if (e == cudaSuccess && need_aux)
+            e = cudaMallocFromPoolAsync(&a->aux, sizeof(double) * 4 * (size_t)h.stride, b->pool, b->stream);
         if (e != cudaSuccess) {
-            if (a->mem) cudaFree(a->mem);
+            if (a->mem) cudaFreeAsync(a->mem, b->stream);
             delete a;
             cudaGetLastError();
             return ITLBM_OK;  // the device is fuller than the budget says: try again next round
         }
         if ((e = case_bind(h, a->mem, per_buf)) != cudaSuccess) {
-            cudaFree(a->mem);
-            if (a->aux) cudaFree(a->aux);
+            cudaFreeAsync(a->mem, b->stream);
+            if (a->aux) cudaFreeAsync(a->aux, b->stream);
             delete a;
             return cuda_fail(e, "state tensor map");
         }
@@ -217,7 +299,13 @@ int admit(itlbm_batch *b) {
         // on the batch stream, which is not ordered after the legacy stream's copies
         e = cudaMemcpyAsync(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream);
         if (p.snapshot.empty()) {
-            if (e == cudaSuccess) e = launch_init(h, b->d_cases + slot, d, b->stream);
+            const size_t len = profile_len(h, d);
+            if (e == cudaSuccess) e = stage_reserve(b, len);
+            if (e == cudaSuccess) {
+                init_profile(h, d, b->stage + b->stage_used);
+                e = launch_init_from(h, b->d_cases + slot, d, b->stage_dev + b->stage_used, b->stream);
+                b->stage_used += len;
+            }
             if (e != cudaSuccess) return cuda_fail(e, "admission");
         } else {
             if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
@@ -261,6 +349,18 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
         cudaMemGetInfo(&fr, &tot);
         b->cfg.hbm_budget = (size_t)(0.9 * (double)fr);
     }
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = b->device;
+        if ((e = cudaMemPoolCreate(&b->pool, &props)) != cudaSuccess) {
+            delete b;
+            return cuda_fail(e, "case memory pool");
+        }
+        cuuint64_t keep = b->cfg.hbm_budget;
+        cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     // launch shape: one CTA per tile of the work table (the grid follows the table and the graph is
     // re-captured when it changes), or, with ctas_per_sm > 0, that many persistent CTAs per SM
     // striding over the table
@@ -292,6 +392,17 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
     }
     cudaEventCreate(&b->ev0);
     cudaEventCreate(&b->ev1);
+    cudaEventCreate(&b->ev2);
+    if ((e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess) {
+        itlbm_batch_destroy(b);
+        return cuda_fail(e, "batch events");
+    }
+    for (int p = 0; p < NTAB; p++)
+        if ((e = cudaStreamCreateWithFlags(&b->side[p], cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&b->ev_join[p], cudaEventDisableTiming)) != cudaSuccess) {
+            itlbm_batch_destroy(b);
+            return cuda_fail(e, "batch streams");
+        }
     b->t0 = std::chrono::steady_clock::now();
     int r = capture_graph(b);
     if (r) {
@@ -308,10 +419,11 @@ void itlbm_batch_destroy(itlbm_batch *b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (Active *a : b->slots)
         if (a) {
-            cudaFree(a->mem);
-            if (a->aux) cudaFree(a->aux);
+            cudaFreeAsync(a->mem, b->stream);
+            if (a->aux) cudaFreeAsync(a->aux, b->stream);
             delete a;
         }
+    if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->d_cases) cudaFree(b->d_cases);
     for (int p = 0; p < NTAB; p++)
@@ -322,7 +434,15 @@ void itlbm_batch_destroy(itlbm_batch *b) {
     diag_free(b->diag);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->ev2) cudaEventDestroy(b->ev2);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (int p = 0; p < NTAB; p++) {
+        if (b->ev_join[p]) cudaEventDestroy(b->ev_join[p]);
+        if (b->side[p]) cudaStreamDestroy(b->side[p]);
+    }
     if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->pool) cudaMemPoolDestroy(b->pool);
+    if (b->stage) cudaFreeHost(b->stage);
     delete b;
 }
 
@@ -353,7 +473,7 @@ int itlbm_batch_save(itlbm_batch *b, long long tag, const char *path) {
 
 int itlbm_batch_submit(itlbm_batch *b, const itlbm_case_desc *d, int n_steps, long long tag) {
     if (!b || !d || n_steps < 1) return fail(ITLBM_E_ARG, "bad argument");
-    if (d->nx < 1 || d->ny < 1 || !(d->tau > 0.0) ||
+    if (d->nx < 1 || d->ny < 1 || !box_tileable(d->nx, d->ny) || !(d->tau > 0.0) ||
         !prec_valid(d->precision) ||
         (d->geometry != ITLBM_GEOM_DROP && d->geometry != ITLBM_GEOM_STRIP) ||
         (d->geometry == ITLBM_GEOM_STRIP && (d->nx != d->ny || (d->p == 0 && d->q == 0))))
@@ -368,15 +488,21 @@ int itlbm_batch_submit(itlbm_batch *b, const itlbm_case_desc *d, int n_steps, lo
 int itlbm_batch_advance(itlbm_batch *b, void *stream) {
     (void)stream;  // the batch runs on its own stream (graphs cannot be captured on the legacy one)
     if (!b) return fail(ITLBM_E_ARG, "NULL batch");
+    ScopeTimer timer(b, b->advance_ms);
     cudaSetDevice(b->device);
-    int r = admit(b);
+    int r;
+    {
+        ScopeTimer t_admit(b, b->admit_ms);
+        r = admit(b);
+    }
     if (r) return r;
     // plan: every case runs to its next diagnostic step, at most `chunk` steps
     const int de = b->cfg.diag_every;
-    int K = 0;
+    int K = 0, hi = -1;
     long long updates = 0;
     for (Active *a : b->slots) {
         if (!a) continue;
+        hi = std::max(hi, a->slot);
         int d = ((a->next_step + de - 1) / de) * de;  // next multiple of diag_every >= next_step
         if (d > a->n_steps - 1) d = a->n_steps - 1;
         a->chunk_len = std::min(d - a->next_step + 1, b->cfg.chunk);
@@ -389,7 +515,8 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         updates += (long long)a->chunk_len * a->desc.nx * a->desc.ny;
     }
     if (K == 0) return (int)b->events.size();
-    cudaError_t e = cudaMemcpyAsync(b->d_cases, b->h_cases.data(), sizeof(CaseDev) * b->h_cases.size(),
+    // the descriptors up to the highest slot in use (the step kernels read no other)
+    cudaError_t e = cudaMemcpyAsync(b->d_cases, b->h_cases.data(), sizeof(CaseDev) * (size_t)(hi + 1),
                                     cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "case table upload");
     if (b->tables_dirty) {
@@ -414,12 +541,7 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         e = cudaGraphLaunch(b->graph, b->stream);
         if (e != cudaSuccess) return cuda_fail(e, "graph launch");
     } else {
-        for (int k = 0; k < K; k++) {
-            for (int p = 0; p < NTAB; p++)
-                launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
-                            p == 1 && b->march, b->stream);
-        }
-        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "step launches");
+        if ((e = enqueue_steps(b, K)) != cudaSuccess) return cuda_fail(e, "step launches");
     }
     cudaEventRecord(b->ev1, b->stream);
     b->replays++;
@@ -457,11 +579,13 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         if (e != cudaSuccess) return cuda_fail(e, "diagnostics");
         measured.push_back(a);
     }
+    cudaEventRecord(b->ev2, b->stream);
     if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "replay");
     if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
     float ms = 0;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->device_ms += ms;
+    if (!measured.empty() && cudaEventElapsedTime(&ms, b->ev1, b->ev2) == cudaSuccess) b->diag_ms += ms;
     if (!measured.empty()) {
         int lo = INT_MAX, hi = -1;
         for (Active *a : measured) {
@@ -531,6 +655,11 @@ int itlbm_batch_stats_get(const itlbm_batch *b, itlbm_batch_stats *out) {
     out->device_ms = b->device_ms;
     out->hbm_used = b->hbm_used;
     out->replays = b->replays;
+    out->captures = b->captures;
+    out->diag_ms = b->diag_ms;
+    out->advance_ms = b->advance_ms;
+    out->admit_ms = b->admit_ms;
+    out->capture_ms = b->capture_ms;
     return ITLBM_OK;
 }
 

@@ -118,11 +118,18 @@ struct CaseDev {
     double rho0;           // FP32 shifted storage: reference density of e_i = f_i - w_i rho0
 };
 
-// A tile of the work table: case index and linear tile index within that case.
+// An entry of the work table: case index and work item within that case.  For the tile kernel the
+// item is the tile's column and row packed as (ty << 16) | tx (no division in the kernel); for the
+// marching kernel it is the linear item index.
 struct TileRef {
     int case_id;
     int tile;
 };
+// Boxes whose tile columns or rows would not fit 16 bits are refused at creation.
+constexpr int MAX_TILE_COORD = 65535;
+inline bool box_tileable(int nx, int ny) {
+    return (nx + TX - 1) / TX <= MAX_TILE_COORD && (ny + TY - 1) / TY <= MAX_TILE_COORD;
+}
 
 // ---- kernel launchers (defined in the .cu files) -------------------------------------------
 cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
@@ -148,6 +155,7 @@ size_t march_smem_bytes();
 // state block: pointers and, for the marching kernel, the tensor map.
 void case_layout(CaseDev &h, int nx, int ny, int prec, bool march);
 int case_items(const CaseDev &h);
+int item_code(const CaseDev &h, int k);  // the TileRef::tile of work item k
 cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf);
 // The FP32 kernel the library uses: the tile kernel, or the marching kernel with ITLBM_STEP_KERNEL=march.
 bool march_default();
@@ -156,7 +164,11 @@ cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntil
                         const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
                         cudaStream_t s);
 cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
-                        cudaStream_t s);
+                        cudaStream_t s);  // single cases: stages the profile, waits
+size_t profile_len(const CaseDev &c, const itlbm_case_desc &d);
+void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof);  // host, profile_len values
+cudaError_t launch_init_from(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
+                             const double *prof, cudaStream_t s);  // prof readable by the device
 // Export populations to FP64 AoS (reference layout).  which = 0: state of buffer `cur`;
 // which = 1: post-collision of the last step (gathered from buffer `cur`).
 cudaError_t launch_export(const CaseDev *c_dev, int nx, int ny, int cur, int which, double *fR,

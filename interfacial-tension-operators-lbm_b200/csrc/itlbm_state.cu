@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 namespace itlbm {
@@ -169,54 +170,80 @@ int grid_for(long long n, int threads) {
 
 }  // namespace
 
+// Length of the initial profile of a case: one value per node for a drop, one per distance class
+// for a strip.
+size_t profile_len(const CaseDev &c, const itlbm_case_desc &d) {
+    return d.geometry == ITLBM_GEOM_DROP ? (size_t)c.nx * c.ny : (size_t)c.nx;
+}
+
 // Host side of the initial profile: the expressions of Initial_conditions.cpp:66-86 (drop) and
 // Imm_INCL.cpp:310-324 (strip), evaluated with the host's libm like the reference does.
-cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
-                        cudaStream_t s) {
+void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof) {
     const long long n = (long long)c.nx * c.ny;
-    std::vector<double> prof;
     if (d.geometry == ITLBM_GEOM_DROP) {
         const double radius = d.radius > 0.0 ? d.radius : 0.25 * (double)d.nx;
         const double k_perfil = d.k_profile;
         const int x0 = c.nx / 2, y0 = c.ny / 2;
-        prof.resize(n);
-        for (int y = 0; y < c.ny; y++)
-            for (int x = 0; x < c.nx; x++) {
-                const double dx = (double)(x - x0), dy = (double)(y - y0), dz = 0.0;
-                const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
-                double phi;
-                if (k_perfil > 0.0) {
-                    double arg = k_perfil * (r - radius);
-                    if (arg > 60.0) arg = 60.0;
-                    if (arg < -60.0) arg = -60.0;
-                    phi = 1.0 / (1.0 + std::exp(arg));
-                } else {
-                    phi = (r < radius) ? 1.0 : 0.0;
+        auto rows = [&](int ya, int yb) {
+            for (int y = ya; y < yb; y++)
+                for (int x = 0; x < c.nx; x++) {
+                    const double dx = (double)(x - x0), dy = (double)(y - y0), dz = 0.0;
+                    const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+                    double phi;
+                    if (k_perfil > 0.0) {
+                        double arg = k_perfil * (r - radius);
+                        if (arg > 60.0) arg = 60.0;
+                        if (arg < -60.0) arg = -60.0;
+                        phi = 1.0 / (1.0 + std::exp(arg));
+                    } else {
+                        phi = (r < radius) ? 1.0 : 0.0;
+                    }
+                    prof[(size_t)y * c.nx + x] = phi;
                 }
-                prof[(size_t)y * c.nx + x] = phi;
-            }
+        };
+        // every node is independent: large boxes are split by rows over host threads
+        const int nthr = n < (1 << 16) ? 1 : (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+        if (nthr == 1) {
+            rows(0, c.ny);
+        } else {
+            std::vector<std::thread> pool;
+            for (int t = 0; t < nthr; t++)
+                pool.emplace_back(rows, (int)((long long)c.ny * t / nthr), (int)((long long)c.ny * (t + 1) / nthr));
+            for (auto &th : pool) th.join();
+        }
     } else {
         const int N = c.nx, p = d.p, q = d.q;
         const double m = std::sqrt((double)(p * p + q * q));
         const double k = 2.0 * std::log(9.0) / 3.45;
-        prof.resize(N);
         for (long long s2 = 0; s2 < N; s2++) {
             const double dred = (2 * s2 < N) ? std::min((double)s2, 0.5 * N - s2) / m
                                              : -std::min(s2 - 0.5 * N, (double)(N - s2)) / m;
             prof[s2] = 1.0 / (1.0 + std::exp(-k * dred));
         }
     }
+}
+
+// The initial state from a profile already in memory the device can read (device memory, or
+// mapped pinned host memory, which the kernel reads across the host link once per value).
+cudaError_t launch_init_from(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
+                             const double *prof, cudaStream_t s) {
+    const long long n = (long long)c.nx * c.ny;
+    k_init<<<grid_for(n, 256), 256, 0, s>>>(c_dev, d.geometry, prof, d.v0, d.rho_R, d.rho_B, d.p, d.q);
+    return cudaGetLastError();
+}
+
+// Single cases: the profile is staged through device memory and the call waits for the state.
+cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
+                        cudaStream_t s) {
+    std::vector<double> prof(profile_len(c, d));
+    init_profile(c, d, prof.data());
     double *dprof = nullptr;
     cudaError_t e = cudaMalloc(&dprof, sizeof(double) * prof.size());
     if (e != cudaSuccess) return e;
     // on the launch stream: a pageable copy may return before its data has reached the device, and
     // a non-blocking stream is not ordered after the legacy stream
     e = cudaMemcpyAsync(dprof, prof.data(), sizeof(double) * prof.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) {
-        k_init<<<grid_for(n, 256), 256, 0, s>>>(c_dev, d.geometry, dprof, d.v0, d.rho_R, d.rho_B,
-                                                d.p, d.q);
-        e = cudaGetLastError();
-    }
+    if (e == cudaSuccess) e = launch_init_from(c, c_dev, d, dprof, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(dprof);
     return e;

@@ -75,6 +75,13 @@ __device__ __forceinline__ int wrapi(int a, int n) {
     int r = a % n;
     return r < 0 ? r + n : r;
 }
+// a in [-HMAX, n + HMAX) -> a mod n by compare and add; only boxes narrower than the halo take the
+// division
+__device__ __forceinline__ int wrap_near(int a, int n) {
+    int r = a < 0 ? a + n : (a >= n ? a - n : a);
+    if ((unsigned)r >= (unsigned)n) r = wrapi(r, n);
+    return r;
+}
 
 template <class S>
 struct SmemT {
@@ -93,22 +100,27 @@ __device__ __forceinline__ float phase_of(float drho, float D, const CaseDev &c)
     return D / ((float)c.rho0 + drho);
 }
 
-// ring position r -> staged-tile coordinates (px, py) for a halo of H around the TX x TY interior;
-// consecutive r run along x in the top and bottom bands, so loads of consecutive r coalesce
+// ring position r -> staged-tile coordinates (px, py) for a halo of H (1 or 2) around the TX x TY
+// interior; consecutive r run along x in the top and bottom bands, so loads of consecutive r
+// coalesce.  The divisions by the band width W are a multiply by ceil(2^16 / W) and a shift, exact
+// for r < 2^16 / W (r stays below 2 x 176 here).
 __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
-    const int W = TX + 2 * H;
+    constexpr int W1 = TX + 2, W2 = TX + 4;
+    constexpr int M1 = (65536 + W1 - 1) / W1, M2 = (65536 + W2 - 1) / W2;
+    static_assert(2 * ((TX + 4) * (TY + 4) - TX * TY) * M1 < (1 << 30), "ring index range");
+    const int W = TX + 2 * H, M = H == 1 ? M1 : M2;
     const int nTop = H * W;
-    if (r < nTop) {
-        py = HMAX - H + r / W;
-        px = HMAX - H + r % W;
-    } else if (r < 2 * nTop) {
-        r -= nTop;
-        py = HMAX + TY + r / W;
-        px = HMAX - H + r % W;
+    if (r < 2 * nTop) {
+        const int band = r < nTop ? 0 : 1;
+        r -= band * nTop;
+        const int q = (r * M) >> 16;
+        py = band ? HMAX + TY + q : HMAX - H + q;
+        px = HMAX - H + (r - q * W);
     } else {
         r -= 2 * nTop;
-        py = HMAX + r / (2 * H);
-        const int k = r % (2 * H);
+        const int q = H == 1 ? (r >> 1) : (r >> 2);  // r / (2 H)
+        const int k = r - q * 2 * H;
+        py = HMAX + q;
         px = k < H ? HMAX - H + k : HMAX + TX + (k - H);
     }
 }
@@ -130,7 +142,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     const int lx = tid % TX, ly = tid / TX;
     const int nx = c.nx, ny = c.ny, pitch = c.pitch;
     const long long stride = c.stride;
-    const int x0 = (tile % c.tiles_x) * TX, y0 = (tile / c.tiles_x) * TY;
+    const int x0 = (int)((unsigned)tile & 0xFFFFu) * TX, y0 = (int)((unsigned)tile >> 16) * TY;
     const int xe = min(x0 + TX, nx), ye = min(y0 + TY, ny);  // end of the valid interior
     const int H = c.halo;
     const int cur = (c.parity0 + k) & 1;
@@ -144,7 +156,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     S f[NP], sa = S(0), sb = S(0);
     double sbd = 0.0;
     if (x < xe + H && y < ye + H) {
-        const int xw = valid ? x : wrapi(x, nx), yw = valid ? y : wrapi(y, ny);
+        const int xw = valid ? x : wrap_near(x, nx), yw = valid ? y : wrap_near(y, ny);
         const long long off = (long long)yw * pitch + xw;
         S a[NP], b[NP];
 #pragma unroll
@@ -172,12 +184,12 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     }
     const int nring = (TX + 2 * H) * (TY + 2 * H) - TX * TY;
     for (int it = tid; it < 2 * nring; it += STEP_THREADS) {
-        const int colour = it / nring, r = it - colour * nring;
+        const int colour = it >= nring ? 1 : 0, r = it - colour * nring;
         int px, py;
         ring_pos(r, H, px, py);
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
         if (gx < xe + H && gy < ye + H) {
-            const long long off = (long long)wrapi(gy, ny) * pitch + wrapi(gx, nx);
+            const long long off = (long long)wrap_near(gy, ny) * pitch + wrap_near(gx, nx);
             const S *p = src + (long long)(colour * NP) * stride + off;
             S v[NP];
 #pragma unroll

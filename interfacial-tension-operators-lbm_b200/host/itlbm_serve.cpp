@@ -353,7 +353,9 @@ int main(int argc, char **argv) {
            << ", \"node_updates\": " << st.node_updates << ", \"device_ms\": " << st.device_ms
            << ", \"wall_s\": " << wall << ", \"mlups_wall\": " << st.node_updates / wall / 1e6
            << ", \"mlups_device\": " << (st.device_ms > 0 ? st.node_updates / (st.device_ms * 1e3) : 0.0)
-           << ", \"hbm_used\": " << st.hbm_used << "}\n";
+           << ", \"diag_ms\": " << st.diag_ms << ", \"advance_ms\": " << st.advance_ms
+           << ", \"admit_ms\": " << st.admit_ms << ", \"capture_ms\": " << st.capture_ms
+           << ", \"captures\": " << st.captures << ", \"hbm_used\": " << st.hbm_used << "}\n";
         std::string stats = js.str();
         for (size_t pos; (pos = stats.find("nan")) != std::string::npos;) stats.replace(pos, 3, "null");
         write_text(join(spool, "serve_stats.json"), stats);

@@ -142,6 +142,9 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     const int lx = tid % TX, ly = tid / TX;
     const int nx = c.nx, ny = c.ny, pitch = c.pitch;
     const long long stride = c.stride;
+    // plane q of a buffer (uniform across the CTA); offsets within a plane are 32-bit (a plane holds
+    // fewer than 2^31 elements: boxes are capped at 2^30 nodes and 65535 tile rows)
+    auto plane = [stride](auto *buf, int q) { return buf + (long long)q * stride; };
     const int x0 = (int)((unsigned)tile & 0xFFFFu) * TX, y0 = (int)((unsigned)tile >> 16) * TY;
     const int xe = min(x0 + TX, nx), ye = min(y0 + TY, ny);  // end of the valid interior
     const int H = c.halo;
@@ -157,12 +160,12 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     double sbd = 0.0;
     if (x < xe + H && y < ye + H) {
         const int xw = valid ? x : wrap_near(x, nx), yw = valid ? y : wrap_near(y, ny);
-        const long long off = (long long)yw * pitch + xw;
+        const int off = yw * pitch + xw;
         S a[NP], b[NP];
 #pragma unroll
-        for (int i = 0; i < NP; i++) a[i] = ldg<LD_OWN>(src + (long long)i * stride + off);
+        for (int i = 0; i < NP; i++) a[i] = ldg<LD_OWN>(plane(src, i) + off);
 #pragma unroll
-        for (int i = 0; i < NP; i++) b[i] = ldg<LD_OWN>(src + (long long)(NP + i) * stride + off);
+        for (int i = 0; i < NP; i++) b[i] = ldg<LD_OWN>(plane(src, NP + i) + off);
 #pragma unroll
         for (int i = 0; i < NP; i++) sa = sa + a[i];
 #pragma unroll
@@ -189,11 +192,10 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         ring_pos(r, H, px, py);
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
         if (gx < xe + H && gy < ye + H) {
-            const long long off = (long long)wrap_near(gy, ny) * pitch + wrap_near(gx, nx);
-            const S *p = src + (long long)(colour * NP) * stride + off;
+            const int off = wrap_near(gy, ny) * pitch + wrap_near(gx, nx);
             S v[NP];
 #pragma unroll
-            for (int i = 0; i < NP; i++) v[i] = ldg<LD_RING>(p + (long long)i * stride);
+            for (int i = 0; i < NP; i++) v[i] = ldg<LD_RING>(plane(src, colour * NP + i) + off);
             S acc = S(0);
 #pragma unroll
             for (int i = 0; i < NP; i++) acc = acc + v[i];
@@ -279,7 +281,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             const int ex = FOLD ? kx(i) : cx(i), ey = FOLD ? ky(i) : cy(i);
             const int xd = ex == 0 ? x : (ex > 0 ? xp : xm);
             const int yd = ey == 0 ? y : (ey > 0 ? yp : ym);
-            return (long long)yd * pitch + xd;
+            return yd * pitch + xd;
         };
         bool skip;
         if constexpr (FOLD) {
@@ -296,15 +298,15 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                     split_fold_pair<K>(rc, f[K], f[K + 1], rho0, dK, dJ);
                     dsum += (double)dK;
                     dsum += (double)dJ;
-                    const long long oK = dst_off(K), oJ = dst_off(K + 1);
-                    stg(&dst[(long long)K * stride + oK], f[K]);
-                    stg(&dst[(long long)(NK + K) * stride + oK], dK);
-                    stg(&dst[(long long)(K + 1) * stride + oJ], f[K + 1]);
-                    stg(&dst[(long long)(NK + K + 1) * stride + oJ], dJ);
+                    const int oK = dst_off(K), oJ = dst_off(K + 1);
+                    stg(plane(dst, K) + oK, f[K]);
+                    stg(plane(dst, NK + K) + oK, dK);
+                    stg(plane(dst, K + 1) + oJ, f[K + 1]);
+                    stg(plane(dst, NK + K + 1) + oJ, dJ);
                 });
-                const long long o0 = dst_off(0);
-                stg(&dst[o0], f[0]);
-                stg(&dst[(long long)NK * stride + o0], (float)(sbd - dsum));
+                const int o0 = dst_off(0);
+                stg(dst + o0, f[0]);
+                stg(plane(dst, NK) + o0, (float)(sbd - dsum));
             }
         } else if constexpr (std::is_same<S, double>::value) {
             Recolour64 rc;
@@ -316,9 +318,9 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                     constexpr int i = decltype(I)::value;
                     double r, b;
                     split64<i>(rc, f[i], r, b);
-                    const long long o = dst_off(i);
-                    stg(&dst[(long long)i * stride + o], r);
-                    stg(&dst[(long long)(NV + i) * stride + o], b);
+                    const int o = dst_off(i);
+                    stg(plane(dst, i) + o, r);
+                    stg(plane(dst, NV + i) + o, b);
                 });
             }
         } else {
@@ -339,24 +341,24 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                     split32_pair<i>(rc, f[i], f[i + 1], rho0, di, dj);
                     dsum += (double)di;
                     dsum += (double)dj;
-                    const long long oi = dst_off(i), oj = dst_off(i + 1);
-                    stg(&dst[(long long)i * stride + oi], f[i]);
-                    stg(&dst[(long long)(NV + i) * stride + oi], di);
-                    stg(&dst[(long long)(i + 1) * stride + oj], f[i + 1]);
-                    stg(&dst[(long long)(NV + i + 1) * stride + oj], dj);
+                    const int oi = dst_off(i), oj = dst_off(i + 1);
+                    stg(plane(dst, i) + oi, f[i]);
+                    stg(plane(dst, NV + i) + oi, di);
+                    stg(plane(dst, i + 1) + oj, f[i + 1]);
+                    stg(plane(dst, NV + i + 1) + oj, dj);
                 });
-                const long long o0 = dst_off(0);
-                stg(&dst[o0], f[0]);
-                stg(&dst[(long long)NV * stride + o0], (float)(sbd - dsum));
+                const int o0 = dst_off(0);
+                stg(dst + o0, f[0]);
+                stg(plane(dst, NV) + o0, (float)(sbd - dsum));
             }
         }
         if (skip) {  // rho <= 1e-30: the site is streamed unchanged (Operadores_tensao.cpp:347)
-            const long long off = (long long)y * pitch + x;
+            const int off = y * pitch + x;
             sfor<0, NP>([&](auto I) {
                 constexpr int i = decltype(I)::value;
-                const long long o = dst_off(i);
-                dst[(long long)i * stride + o] = src[(long long)i * stride + off];
-                dst[(long long)(NP + i) * stride + o] = src[(long long)(NP + i) * stride + off];
+                const int o = dst_off(i);
+                plane(dst, i)[o] = plane(src, i)[off];
+                plane(dst, NP + i)[o] = plane(src, NP + i)[off];
             });
         }
 

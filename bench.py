@@ -63,8 +63,8 @@ def load_package():
 PEAKS = REPO / "MEASURED_PEAKS.json"
 # HBM traffic per node of one FP32 step launch, dram__bytes_read.sum + dram__bytes_write.sum from one
 # ncu capture each: a launch over the 600-case batch (12.41 GB for 39 127 049 nodes) and a launch over
-# a 2048^2 drop (1239.1 MB for 4 194 304 nodes).
-TRAFFIC_B_PER_NODE = {"batch600": 12410280448 / 39127049, "single": 1239080192 / 4194304}
+# a 2048^2 drop (1234.7 MB for 4 194 304 nodes).
+TRAFFIC_B_PER_NODE = {"batch600": 12406374400 / 39127049, "single": 1234656256 / 4194304}
 HBM_FALLBACK = 6650.0
 
 

@@ -1,4 +1,5 @@
 // case_io.cpp -- case-folder inputs and outputs (see case_io.h).
+#include <cctype>
 #include "case_io.h"
 
 #include <cmath>
@@ -199,6 +200,24 @@ bool write_perfil(const std::string &path, int N, int p, int q, const std::vecto
             if (std::fabs(dd) < 12.0) fp << dd << " " << rR[k] / rho << " " << rho << " " << ux[k] << " " << uy[k] << "\n";
         }
     return true;
+}
+
+int precision_word(const char *word, int dflt) {
+    if (!word) return dflt;
+    std::string w(word);
+    for (char &ch : w) ch = (char)std::tolower((unsigned char)ch);
+    if (w == "fp64") return ITLBM_PREC_F64;
+    if (w == "fp32") return ITLBM_PREC_F32;
+    if (w == "fold") return ITLBM_PREC_F32_FOLD;
+    return dflt;
+}
+
+const char *precision_label(int prec) {
+    switch (prec) {
+        case ITLBM_PREC_F32: return "FP32 ( f - w rho0 , f_R - f_B )";
+        case ITLBM_PREC_F32_FOLD: return "FP32, nove classes no plano ( f - w rho0 , f_R - f_B )";
+        default: return "FP64";
+    }
 }
 
 }  // namespace itlbm_host

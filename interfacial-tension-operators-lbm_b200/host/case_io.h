@@ -55,6 +55,11 @@ bool write_vtk_velocity(const std::string &path, int nx, int ny, const double *u
 
 std::string join(const std::string &dir, const std::string &file);
 
+// Storage form from an ITLBM_PRECISION word: "fp64", "fp32" or "fold" (either case); a null or other
+// word gives `dflt`.  precision_label is the "precisao" line of the programs' banner.
+int precision_word(const char *word, int dflt);
+const char *precision_label(int prec);
+
 // dist_central (Imm_INCL.cpp:74-83): signed distance to the central interface, > 0 on the red side
 double dist_central(int x, int y, int p, int q, int N);
 

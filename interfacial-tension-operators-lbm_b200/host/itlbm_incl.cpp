@@ -3,7 +3,8 @@
 // Same file contract as Imm_INCL.cpp:192-473: reads data_in.txt, operador.txt, inclinacao.txt and the
 // geometry file (an N x N x 1 all-fluid box); writes dat_out.txt, inclinada.dat every 500 steps and at
 // the last step, perfil.dat at the last step and resumo.dat.  Exit code 1 on invalid input.
-// ITLBM_PRECISION=fp32 selects the FP32 shifted storage; ITLBM_DEVICE selects the CUDA device.
+// ITLBM_PRECISION=fp32 selects the FP32 shifted storage and =fold its nine-class in-plane fold;
+// ITLBM_DEVICE selects the CUDA device.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -70,8 +71,7 @@ int main(int argc, char **argv) {
     const double A_in = din.A_fact;
     const bool forca = op.tipo >= ITLBM_OP_F1;
     const double sigma_nominal = forca ? A_in : 4.0 / 9.0 * A_in * tau;
-    const char *prec_env = std::getenv("ITLBM_PRECISION");
-    const bool fp32 = prec_env && (std::strcmp(prec_env, "fp32") == 0 || std::strcmp(prec_env, "FP32") == 0);
+    const int prec = precision_word(std::getenv("ITLBM_PRECISION"), ITLBM_PREC_F64);
     if (const char *dev = std::getenv("ITLBM_DEVICE")) cudaSetDevice(std::atoi(dev));
 
     std::cout << "\nInterface plana inclinada -- arcabouco comum ( D3Q19, BGK, Latva-Kokko )" << std::endl;
@@ -95,7 +95,7 @@ int main(int argc, char **argv) {
     d.geometry = ITLBM_GEOM_STRIP;
     d.p = p;
     d.q = q;
-    d.precision = fp32 ? ITLBM_PREC_F32 : ITLBM_PREC_F64;
+    d.precision = prec;
     itlbm_case *c = nullptr;
     if (itlbm_case_create(&d, &c) != ITLBM_OK) return die(c, 1, "itlbm_case_create");
 

@@ -8,7 +8,7 @@
 //
 // Extensions (absent files keep the reference's behaviour): gota.txt "R [espessura]" sets the initial
 // radius and the 10-90 % width of the initial profile (0 = sharp step); ITLBM_PRECISION=fp32 selects
-// the FP32 shifted storage; ITLBM_DEVICE selects the CUDA device.
+// the FP32 shifted storage and =fold its nine-class in-plane fold; ITLBM_DEVICE selects the CUDA device.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -73,8 +73,7 @@ int main(int argc, char **argv) {
     const double tau = din.tau_R;
     const double A_in = din.A_fact;
     const double sigma_nominal = forca ? A_in : 4.0 / 9.0 * A_in * tau;
-    const char *prec_env = std::getenv("ITLBM_PRECISION");
-    const bool fp32 = prec_env && (std::strcmp(prec_env, "fp32") == 0 || std::strcmp(prec_env, "FP32") == 0);
+    const int prec = precision_word(std::getenv("ITLBM_PRECISION"), ITLBM_PREC_F64);
     if (const char *dev = std::getenv("ITLBM_DEVICE")) cudaSetDevice(std::atoi(dev));
 
     std::cout << "\nOperadores de tensao interfacial -- arcabouco comum ( D3Q19, BGK, Latva-Kokko )" << std::endl;
@@ -89,7 +88,7 @@ int main(int argc, char **argv) {
     std::cout << "   fat_R_B           = " << A_in << (forca ? "   ( = sigma )" : "   ( = A )") << std::endl;
     std::cout << "   sigma nominal     = " << sigma_nominal << std::endl;
     std::cout << "   v0                = " << v0 << std::endl;
-    std::cout << "   precisao          = " << (fp32 ? "FP32 ( f - w rho0 , f_R - f_B )" : "FP64") << std::endl;
+    std::cout << "   precisao          = " << precision_label(prec) << std::endl;
 
     itlbm_case_desc d{};
     d.nx = nx;
@@ -104,7 +103,7 @@ int main(int argc, char **argv) {
     d.radius = raio_ini;
     d.k_profile = (espessura > 0.0) ? 2.0 * std::log(9.0) / espessura : 0.0;
     d.v0 = v0;
-    d.precision = fp32 ? ITLBM_PREC_F32 : ITLBM_PREC_F64;
+    d.precision = prec;
     itlbm_case *c = nullptr;
     if (itlbm_case_create(&d, &c) != ITLBM_OK) return die(c, 1, "itlbm_case_create");
 

@@ -7,7 +7,7 @@
 // batch (itlbm_batch_*) on the device and admits case folders as they arrive:
 //   * a request is a file <spool>/<name>.req whose first line is the path of a case folder (the
 //     folder rodar_lote.monta writes: data_in.txt, operador.txt, velocity.txt, meio.vtk and, for the
-//     inclined interface, inclinacao.txt); an optional second word "fp64" or "fp32" picks the storage;
+//     inclined interface, inclinacao.txt); an optional second word "fp64", "fp32" or "fold" picks the storage;
 //   * the server renames it <name>.run, validates the folder like Imm_OPS / Imm_INCL (an invalid folder
 //     gets <name>.err with the message, the reference's exit code 1), and submits the case;
 //   * requests that arrive while others run are admitted as memory and slots free up: every round is
@@ -102,7 +102,7 @@ bool same_desc(const itlbm_case_desc &a, const itlbm_case_desc &b) {
 // Reads and validates a case folder like Imm_OPS.cpp:65-135 / Imm_INCL.cpp:192-266.  With
 // `snapshots`, a folder holding a snapshot of the same case that is short of its step count resumes
 // from it (its output files keep their rows up to the snapshot).
-bool prepare(Job &j, bool fp64, bool snapshots, std::string &err) {
+bool prepare(Job &j, int prec, bool snapshots, std::string &err) {
     std::ostringstream log;
     DataIn din;
     if (!read_data(j.dir, din, log)) {
@@ -160,7 +160,7 @@ bool prepare(Job &j, bool fp64, bool snapshots, std::string &err) {
     d.v0 = v0;
     d.p = p;
     d.q = q;
-    d.precision = fp64 ? ITLBM_PREC_F64 : ITLBM_PREC_F32;
+    d.precision = prec;
     j.n_steps = din.n_steps;
     j.nx = nx;
     j.tau = din.tau_R;
@@ -265,8 +265,9 @@ int main(int argc, char **argv) {
             j.name = name;
             j.dir = dir;
             std::string err;
-            const bool fp64 = prec == "fp64" || (prec != "fp32" && fp64_default);
-            if (!prepare(j, fp64, snapshots, err)) {
+            const int prec_code =
+                precision_word(prec.c_str(), fp64_default ? ITLBM_PREC_F64 : ITLBM_PREC_F32);
+            if (!prepare(j, prec_code, snapshots, err)) {
                 write_text(join(spool, name + ".err"), err + "\n");
                 std::remove(run.c_str());
                 failed_inputs++;

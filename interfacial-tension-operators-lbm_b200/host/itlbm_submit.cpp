@@ -4,7 +4,7 @@
 // rodar_lote.py runs (rodar_lote.py:231-243).  It drops a request into the server's spool directory
 // ($ITLBM_SPOOL), waits until the server has finished the case, and exits 0 when the case ran
 // (stable or not, resumo.dat written by the server) or 1 when the folder was invalid (the message of
-// the server on stderr).  ITLBM_PRECISION=fp64 asks for the plain FP64 path; ITLBM_SUBMIT_TIMEOUT
+// the server on stderr).  ITLBM_PRECISION (fp64, fp32 or fold) picks the storage; ITLBM_SUBMIT_TIMEOUT
 // bounds the wait in seconds (default: none).
 #include <chrono>
 #include <climits>

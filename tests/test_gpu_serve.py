@@ -75,3 +75,32 @@ def test_served_equals_alone_and_overlaps(tmp_path):
     import json
     stats = json.loads((spool / "serve_stats.json").read_text())
     assert stats["completed"] == len(cases) and stats["invalid"] == 1 and stats["p99_s"] > 0
+
+
+def test_fold_word_served_and_alone(tmp_path):
+    """ITLBM_PRECISION=fold picks the nine-class FP32 storage through the server and through itlbm_ops
+    alike (the same bytes), and its Laplace jump, tension and area radius stay within the FP32 bars of
+    the FP64 run of the same folder."""
+    from test_dropin import _rows
+    spool = tmp_path / "spool"
+    spool.mkdir()
+    server = subprocess.Popen([str(BIN / "itlbm_serve"), str(spool), "--idle-exit", "2", "--chunk", "250"],
+                              stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+    try:
+        served = make_case(tmp_path / "served", "P3 0.5", 0.225, 0.8, 48, 1001)
+        r = submit(served, spool, prec="fold")
+        assert r.returncode == 0, r.stderr
+    finally:
+        server.wait(timeout=120)
+    alone = make_case(tmp_path / "alone", "P3 0.5", 0.225, 0.8, 48, 1001)
+    r = run(BIN / "itlbm_ops", alone, {"ITLBM_PRECISION": "fold"})
+    assert r.returncode == 0 and "nove classes" in r.stdout
+    assert (served / "laplace.dat").read_text() == (alone / "laplace.dat").read_text()
+    ref = make_case(tmp_path / "fp64", "P3 0.5", 0.225, 0.8, 48, 1001)
+    assert run(BIN / "itlbm_ops", ref).returncode == 0
+    rows_f, rows_d = _rows(alone / "laplace.dat"), _rows(ref / "laplace.dat")
+    assert len(rows_f) == len(rows_d) == 3
+    for a, b in zip(rows_f[1:], rows_d[1:]):  # steps 500 and 1000
+        assert abs(float(a[6]) - float(b[6])) <= 5e-3 * abs(float(b[6]))  # delta_p
+        assert abs(float(a[7]) - float(b[7])) <= 5e-3 * abs(float(b[7]))  # sigma
+        assert abs(float(a[1]) - float(b[1])) <= 2e-4 * float(b[1])  # raio_area

@@ -16,7 +16,10 @@ constexpr int NV = 19;
 
 // Tile of the fused step: TX x TY interior nodes, one per thread; the phase field is staged with a
 // halo of up to HMAX nodes (1 for P1/P3/F3, 2 for F1/F2).
-constexpr int TX = 32;
+#ifndef ITLBM_TILE_COLS
+#define ITLBM_TILE_COLS 32
+#endif
+constexpr int TX = ITLBM_TILE_COLS;
 #ifndef ITLBM_TILE_ROWS
 #define ITLBM_TILE_ROWS 8
 #endif

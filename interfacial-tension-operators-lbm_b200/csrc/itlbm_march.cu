@@ -198,16 +198,18 @@ __device__ __forceinline__ void aux_pass(const CaseDev &c, const Item &it, int r
         const int r = ra + q / AW, ax = q % AW;
         const int pr = r - it.y0 + PR, bx = ax + 3;  // phi column of aux column ax
         auto phi = [&](int dx, int dy) { return sm.phi[(pr + dy) & (PR - 1)][bx + dx]; };
-        float g0, g1, g2;
-        iso_grad_f32(phi, g0, g1, g2);
+        float g0, g1;
+        mediator_grad_fold(phi, g0, g1);  // the class form, as the tile kernel (g_z = 0 on the slab)
+        g0 = -g0;
+        g1 = -g1;
         float *a = sm.aux[(r - it.y0 + NR) & (NR - 1)][ax];
         if (c.tipo == ITLBM_OP_F1) {
-            aux_normal(g0, g1, g2, a);
+            aux_normal_plane(g0, g1, a);
             a[3] = g0;
             a[4] = g1;
-            a[5] = g2;
+            a[5] = 0.f;
         } else {
-            aux_stress(g0, g1, g2, (float)c.sigma, a);
+            aux_stress_plane(g0, g1, (float)c.sigma, a);
         }
     }
 }
@@ -233,26 +235,27 @@ __device__ __forceinline__ void collide_row(const CaseDev &c, const Item &it, in
     const float sb = sm.Df[rr][lane];
     const int pr = r - it.y0 + PR, bx = lane + 4;
     auto phi = [&](int dx, int dy) { return sm.phi[(pr + dy) & (PR - 1)][bx + dx]; };
-    float gmx, gmy, gmz;
-    mediator_grad_f32(phi, gmx, gmy, gmz);
+    float gmx, gmy;
+    mediator_grad_fold(phi, gmx, gmy);
+    const float gmz = 0.f;
     float Fx = 0.f, Fy = 0.f, Fz = 0.f;
     const bool force = tipo >= ITLBM_OP_F1;
     if (tipo == ITLBM_OP_F1 || tipo == ITLBM_OP_F2) {
         const int ar = r - it.y0 + NR, ax = lane + 1;
         auto aux = [&](int dx, int dy) -> const float * { return sm.aux[(ar + dy) & (NR - 1)][ax + dx]; };
         if (tipo == ITLBM_OP_F1) {
-            const float kappa = curvature_at<float>(aux);
+            const float kappa = curvature_plane(aux);
             const float hs = (0.5f * (float)c.sigma) * kappa;
             const float *g = aux(0, 0);
             Fx = hs * g[3];
             Fy = hs * g[4];
             Fz = hs * g[5];
         } else {
-            stress_div_at<float>(aux, Fx, Fy, Fz);
+            stress_div_plane(aux, Fx, Fy);
         }
     } else if (tipo == ITLBM_OP_F3) {
         const float g0 = -gmx, g1 = -gmy, g2 = -gmz;  // the isotropic gradient, exactly
-        const float mu = chem_pot_f32(phi, (float)c.kf, (float)c.bf);
+        const float mu = chem_pot_fold(phi, (float)c.kf, (float)c.bf);
         Fx = mu * g0;
         Fy = mu * g1;
         Fz = mu * g2;

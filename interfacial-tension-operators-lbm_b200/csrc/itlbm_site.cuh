@@ -484,6 +484,56 @@ __device__ __forceinline__ void mediator_grad_fold(P phi, float &gx, float &gy) 
     gx = ax;
     gy = ay;
 }
+// FP32 F1 / F2 auxiliaries by class.  On the slab g_z = 0, so n_z = 0 and the stress has no xz, yz
+// components, and the z-moving members of a class read the same in-plane node with opposite c_z: in
+// curvature_at and stress_div_at they cancel in pairs, and what is left is the class sum.
+//   F1: n = (n_x, n_y) in a[0..1];  kappa = -3 sum_K W_K (e_K . n(x + e_K))
+//   F2: (T_xx, T_yy, T_xy) in a[0..2];  F_a = 3 sum_K W_K (T_ax e_Kx + T_ay e_Ky)(x + e_K), F_z = 0
+__device__ __forceinline__ void aux_normal_plane(float gx, float gy, float *a) {
+    const float m = sqrtf(gx * gx + gy * gy);
+    const float inv = (m > 1.0e-12f) ? 1.0f / m : 0.0f;
+    a[0] = gx * inv;
+    a[1] = gy * inv;
+}
+__device__ __forceinline__ void aux_stress_plane(float gx, float gy, float sigma, float *a) {
+    const float m = sqrtf(gx * gx + gy * gy);
+    const float h = 0.5f * sigma;
+    const float inv = (m > 1.0e-30f) ? 1.0f / m : 0.0f;
+    a[0] = h * (m - gx * gx * inv);
+    a[1] = h * (m - gy * gy * inv);
+    a[2] = -h * gx * gy * inv;
+}
+template <class A>
+__device__ __forceinline__ float curvature_plane(A aux) {
+    float d1 = 0.f, d2 = 0.f;
+    sfor<1, NK>([&](auto KC) {
+        constexpr int K = decltype(KC)::value;
+        const float *v = aux(kx(K), ky(K));
+        const float s = kdot<K>(v[0], v[1]);
+        if constexpr (kk(K) == 1) d1 += s;
+        else d2 += s;
+    });
+    return -3.0f * (d1 * (1.0f / 9.0f) + d2 * (1.0f / 36.0f));
+}
+template <class A>
+__device__ __forceinline__ void stress_div_plane(A aux, float &Fx, float &Fy) {
+    float x1 = 0.f, y1 = 0.f, x2 = 0.f, y2 = 0.f;
+    sfor<1, NK>([&](auto KC) {
+        constexpr int K = decltype(KC)::value;
+        const float *t = aux(kx(K), ky(K));
+        const float fx = kdot<K>(t[0], t[2]), fy = kdot<K>(t[2], t[1]);
+        if constexpr (kk(K) == 1) {
+            x1 += fx;
+            y1 += fy;
+        } else {
+            x2 += fx;
+            y2 += fy;
+        }
+    });
+    Fx = 3.0f * (x1 * (1.0f / 9.0f) + x2 * (1.0f / 36.0f));
+    Fy = 3.0f * (y1 * (1.0f / 9.0f) + y2 * (1.0f / 36.0f));
+}
+
 // F3 chemical potential, lap = 6 sum_K W_K (phi(x + e_K) - phi)
 template <class P>
 __device__ __forceinline__ float chem_pot_fold(P phi, float kf, float bf) {
@@ -496,50 +546,6 @@ __device__ __forceinline__ float chem_pot_fold(P phi, float kf, float bf) {
         else l2 += s;
     });
     const float lap = 6.0f * (fmaf(-4.0f, ph, l1) * (1.0f / 9.0f) + fmaf(-4.0f, ph, l2) * (1.0f / 36.0f));
-    return 4.0f * bf * ph * (ph * ph - 1.0f) - kf * lap;
-}
-
-// FP32 stencils by pairs (the FP64 path uses the per-direction forms below, in the reference's
-// order).  Mediator momentum sum_i c_i w_i 3 phi(x - c_i); the isotropic gradient
-// 3 sum_i w_i c_i phi(x + c_i) is its exact negative.
-template <class P>
-__device__ __forceinline__ void mediator_grad_f32(P phi, float &gx, float &gy, float &gz) {
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    sfor<0, 9>([&](auto M) {
-        constexpr int i = 2 * decltype(M)::value + 1;
-        constexpr float w3 = 3.0f * wgt<float>(i);
-        const float dphi = w3 * (phi(-cx(i), -cy(i)) - phi(cx(i), cy(i)));
-        if constexpr (cx(i) == 1) ax += dphi;
-        if constexpr (cx(i) == -1) ax -= dphi;
-        if constexpr (cy(i) == 1) ay += dphi;
-        if constexpr (cy(i) == -1) ay -= dphi;
-        if constexpr (cz(i) == 1) az += dphi;
-        if constexpr (cz(i) == -1) az -= dphi;
-    });
-    gx = ax;
-    gy = ay;
-    gz = az;
-}
-template <class P>
-__device__ __forceinline__ void iso_grad_f32(P phi, float &gx, float &gy, float &gz) {
-    mediator_grad_f32(phi, gx, gy, gz);
-    gx = -gx;
-    gy = -gy;
-    gz = -gz;
-}
-// F3 chemical potential mu = 4 b phi (phi^2 - 1) - k lap phi, lap = 6 sum_i w_i (phi(x + c_i) - phi)
-template <class P>
-__device__ __forceinline__ float chem_pot_f32(P phi, float kf, float bf) {
-    const float ph = phi(0, 0);
-    float l1 = 0.f, l2 = 0.f;
-    sfor<0, 9>([&](auto M) {
-        constexpr int i = 2 * decltype(M)::value + 1;
-        const float s = phi(cx(i), cy(i)) + phi(-cx(i), -cy(i));
-        if constexpr (cc(i) == 1) l1 += s;
-        else l2 += s;
-    });
-    // sum_i w_i (phi_i - ph) = (l1 - 6 ph) / 18 + (l2 - 12 ph) / 36
-    const float lap = 6.0f * (fmaf(-6.0f, ph, l1) * (1.0f / 18.0f) + fmaf(-12.0f, ph, l2) * (1.0f / 36.0f));
     return 4.0f * bf * ph * (ph * ph - 1.0f) - kf * lap;
 }
 

@@ -219,20 +219,22 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             const int gx = x0 - 1 + qx, gy = y0 - 1 + qy;
             if (gx < xe + 1 && gy < ye + 1) {
                 S g0, g1, g2;
-                if constexpr (FOLD) {
+                if constexpr (std::is_same<S, float>::value) {
+                    // FP32 (both storage forms): the in-plane class forms, g_z = 0 on the slab
                     mediator_grad_fold([&](int dx, int dy) { return sm.phi[qy + 1 + dy][qx + 1 + dx]; }, g0, g1);
                     g0 = -g0;  // the isotropic gradient
                     g1 = -g1;
                     g2 = 0.f;
-                } else if constexpr (std::is_same<S, float>::value)
-                    iso_grad_f32([&](int dx, int dy) { return sm.phi[qy + 1 + dy][qx + 1 + dx]; }, g0, g1, g2);
-                else
+                    if (tipo == ITLBM_OP_F1) aux_normal_plane(g0, g1, sm.aux[qy][qx]);
+                    else aux_stress_plane(g0, g1, (float)c.sigma, sm.aux[qy][qx]);
+                } else {
                     iso_grad(sm.phi, qx + 1, qy + 1, g0, g1, g2);
+                    if (tipo == ITLBM_OP_F1) aux_normal(g0, g1, g2, sm.aux[qy][qx]);
+                    else aux_stress(g0, g1, g2, (S)c.sigma, sm.aux[qy][qx]);
+                }
                 sm.g[qy][qx][0] = g0;
                 sm.g[qy][qx][1] = g1;
                 sm.g[qy][qx][2] = g2;
-                if (tipo == ITLBM_OP_F1) aux_normal(g0, g1, g2, sm.aux[qy][qx]);
-                else aux_stress(g0, g1, g2, (S)c.sigma, sm.aux[qy][qx]);
             }
         }
         __syncthreads();
@@ -243,30 +245,35 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         const int px = lx + HMAX, py = ly + HMAX;
         S gmx, gmy, gmz;
         auto phi_at = [&](int dx, int dy) { return sm.phi[py + dy][px + dx]; };
-        if constexpr (FOLD) {
-            mediator_grad_fold(phi_at, gmx, gmy);
+        if constexpr (std::is_same<S, float>::value) {
+            mediator_grad_fold(phi_at, gmx, gmy);  // FP32: class form, g_z = 0 on the slab
             gmz = S(0);
-        } else if constexpr (std::is_same<S, float>::value) mediator_grad_f32(phi_at, gmx, gmy, gmz);
-        else mediator_grad(sm.phi, px, py, gmx, gmy, gmz);
+        } else mediator_grad(sm.phi, px, py, gmx, gmy, gmz);
         S Fx = S(0), Fy = S(0), Fz = S(0);
         const bool force = tipo >= ITLBM_OP_F1;
         if (tipo == ITLBM_OP_F1) {
             const int qx = lx + 1, qy = ly + 1;
-            const S kappa = curvature<S, 6>(sm.aux, qx, qy);
+            S kappa;
+            if constexpr (std::is_same<S, float>::value)
+                kappa = curvature_plane([&](int dx, int dy) { return sm.aux[qy + dy][qx + dx]; });
+            else
+                kappa = curvature<S, 6>(sm.aux, qx, qy);
             const S hs = (S(0.5) * (S)c.sigma) * kappa;
             Fx = hs * sm.g[qy][qx][0];
             Fy = hs * sm.g[qy][qx][1];
             Fz = hs * sm.g[qy][qx][2];
         } else if (tipo == ITLBM_OP_F2) {
-            stress_div<S, 6>(sm.aux, lx + 1, ly + 1, Fx, Fy, Fz);
+            if constexpr (std::is_same<S, float>::value)
+                stress_div_plane([&](int dx, int dy) { return sm.aux[ly + 1 + dy][lx + 1 + dx]; }, Fx, Fy);
+            else
+                stress_div<S, 6>(sm.aux, lx + 1, ly + 1, Fx, Fy, Fz);
         } else if (tipo == ITLBM_OP_F3) {
             S g0, g1, g2, mu;
             if constexpr (std::is_same<S, float>::value) {
                 g0 = -gmx;  // the isotropic gradient is the exact negative of the mediator momentum
                 g1 = -gmy;
                 g2 = -gmz;
-                if constexpr (FOLD) mu = chem_pot_fold(phi_at, (float)c.kf, (float)c.bf);
-                else mu = chem_pot_f32(phi_at, (float)c.kf, (float)c.bf);
+                mu = chem_pot_fold(phi_at, (float)c.kf, (float)c.bf);
             } else {
                 iso_grad(sm.phi, px, py, g0, g1, g2);
                 mu = chem_pot(sm.phi, px, py, (S)c.kf, (S)c.bf);

@@ -1,5 +1,6 @@
 """The batched engine: every case gives the same bits alone and in a mixed batch (cases of
-different sizes, operators, precisions and geometries, admitted at different times), its
+different sizes, operators, storage forms -- FP64, FP32, FP32 fold -- and geometries, admitted at
+different times), its
 diagnostics fall on the reference's steps (every 500 steps and the last), and the admission
 budget is honoured."""
 import math
@@ -22,6 +23,8 @@ MIX = [  # (nx, tipo, chi, A, prec, geometry, pq, steps)
     (33, 13, 0.5, 0.1, 0, 0, (1, 0), 1200),
     (80, 1, 0.5, 0.225, 1, 0, (1, 0), 501),
     (40, 3, 2.0, 0.225, 0, 1, (1, 1), 1),
+    (45, 3, 0.5, 0.225, 2, 0, (1, 0), 650),   # the fold: a third work table, run as its own chain
+    (56, 12, 0.5, 0.1, 2, 1, (1, 2), 900),
 ]
 
 

@@ -22,7 +22,8 @@ def desc(itlbm, nx, tipo, prec, geometry=0, p=1, q=0, v0=0.0):
 
 
 @pytest.mark.parametrize("nx,tipo,prec,geometry,v0", [(64, 3, 0, 0, 0.05), (70, 12, 1, 0, 0.0),
-                                                       (48, 11, 0, 1, 0.0), (53, 13, 1, 0, 0.02)])
+                                                       (48, 11, 0, 1, 0.0), (53, 13, 1, 0, 0.02),
+                                                       (50, 13, 2, 0, 0.01), (44, 11, 2, 1, 0.0)])
 def test_case_resumes_bit_for_bit(gpu, tmp_path, nx, tipo, prec, geometry, v0):
     d = desc(gpu, nx, tipo, prec, geometry, p=2, q=1, v0=v0)
     with gpu.Case(d) as full:

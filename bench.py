@@ -63,8 +63,8 @@ def load_package():
 PEAKS = REPO / "MEASURED_PEAKS.json"
 # HBM traffic per node of one FP32 step launch, dram__bytes_read.sum + dram__bytes_write.sum from one
 # ncu capture each: a launch over the 600-case batch (12.41 GB for 39 127 049 nodes) and a launch over
-# a 2048^2 drop (1234.7 MB for 4 194 304 nodes).
-TRAFFIC_B_PER_NODE = {"batch600": 12406374400 / 39127049, "single": 1234656256 / 4194304}
+# the 4096^2 drop (5.07 GB for 16 777 216 nodes).
+TRAFFIC_B_PER_NODE = {"batch600": 12406374400 / 39127049, "single": 5069217280 / 16777216}
 HBM_FALLBACK = 6650.0
 
 
@@ -437,6 +437,19 @@ def e2e_run(pkg, w, prec, steps):
             "d2h_bytes_per_step": d2h / steps, "wall_s": dt}
 
 
+def host_cpu():
+    """Model name and logical core count of the host."""
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count()
+
+
 def cpu_baseline(threads=0):
     import oracle
     if not oracle.REF_DIR.joinpath("libref_ops_fast.so").exists():
@@ -444,9 +457,16 @@ def cpu_baseline(threads=0):
     nx = 1024
     steps = 8
     mlups, dt, nthr = oracle.time_reference_step(nx, nx, steps=steps, warmup=1, threads=threads)
+    # the same loop on one host thread, on a smaller box (a bounded sample)
+    n1, s1 = 256, 8
+    mlups1, dt1, _ = oracle.time_reference_step(n1, n1, radius=25.0, steps=s1, warmup=1, threads=1)
+    model, ncpu = host_cpu()
     return {"value": mlups, "unit": "MLUPS", "cores": nthr, "kind": "reference",
             "sample": f"reference step loop (Imm_OPS.cpp:252-287, oracle/_ref, its own flags), "
-                      f"{nx}x{nx} drop P3 chi=0.5, {steps} steps, {nthr} OpenMP threads, {dt:.1f} s"}
+                      f"{nx}x{nx} drop P3 chi=0.5, {steps} steps, {nthr} OpenMP threads, {dt:.1f} s",
+            "single_thread": {"value": mlups1, "unit": "MLUPS",
+                              "sample": f"{n1}x{n1} drop P3 chi=0.5, {s1} steps, 1 thread, {dt1:.1f} s"},
+            "host": {"model": model, "logical_cores": ncpu}}
 
 
 METRIC = "MLUPS & % HBM roofline, batched FP32 vs plain FP64 on 1 B200; p99 case latency"

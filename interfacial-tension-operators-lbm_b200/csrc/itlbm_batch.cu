@@ -5,22 +5,27 @@
 // advance together:
 //   * a slot table of per-case descriptors (CaseDev) lives in device memory; each descriptor carries
 //     the case's buffer parity and the number of sub-steps it runs in the current replay;
-//   * a tile work table lists the TX x TY tiles of every active case (one table for FP64 cases, one
-//     for FP32 cases) with its length in device memory;
-//   * one replay is a CUDA graph of `chunk` sub-steps, each one persistent launch per precision whose
-//     CTAs stride over the work table; a case whose chunk is shorter skips its tiles in the remaining
-//     sub-steps.  The graph never changes when cases come and go: only the tables do.
+//   * tile work tables list the TX x TY tiles of every active case, one per storage form (FP64, FP32,
+//     FP32 fold), with their lengths in device memory;
+//   * one replay is a CUDA graph of `chunk` sub-steps: each non-empty table is a chain of launches on
+//     its own stream between a fork and a join, one CTA per table entry (the grid is the table length
+//     rounded up to a bucket); a case whose chunk is shorter skips its tiles in the remaining
+//     sub-steps.  The graph is re-captured only when a table's bucket or storage changes;
+//   * case state comes from a stream-ordered memory pool, and the initial profiles of a round's
+//     admissions are filled by host threads into mapped pinned memory that the init kernel reads.
 // Each case stops at its next diagnostic step (every diag_every steps and its last step, as
 // Imm_OPS.cpp:293), is measured there by the same device diagnostics as a single case, and retires at
 // its step count or when the stop rule of Imm_OPS.cpp:346-352 / Imm_INCL.cpp:428-433 fires.
 #include "itlbm_site.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
 #include <deque>
+#include <thread>
 #include <vector>
 
 namespace itlbm {
@@ -84,6 +89,13 @@ struct itlbm_batch {
     // init kernel reads directly (no device staging buffer to allocate and free per case)
     double *stage = nullptr, *stage_dev = nullptr;
     size_t stage_cap = 0, stage_used = 0;
+    struct InitJob {
+        int slot;
+        itlbm_case_desc d;
+        CaseDev h;
+        size_t off;  // of its profile in the staging buffer
+    };
+    std::vector<InitJob> inits;  // admitted this round, initial state not yet launched
     std::deque<Pending> pending;
     std::vector<Active *> slots;
     std::vector<int> free_slots;
@@ -254,7 +266,45 @@ cudaError_t stage_reserve(itlbm_batch *b, size_t len) {
     return cudaSuccess;
 }
 
-int admit(itlbm_batch *b) {
+// The initial profiles of the cases admitted so far in this round, filled by host threads that take
+// chunks of about 16 K nodes from all of them at once (most boxes are too small to split alone), then
+// their initial-state launches, in admission order.
+cudaError_t flush_inits(itlbm_batch *b) {
+    if (b->inits.empty()) return cudaSuccess;
+    struct Chunk {
+        int job, ya, yb;
+    };
+    std::vector<Chunk> chunks;
+    for (int j = 0; j < (int)b->inits.size(); j++) {
+        const auto &w = b->inits[j];
+        if (w.d.geometry != ITLBM_GEOM_DROP) {
+            chunks.push_back({j, 0, 1});
+            continue;
+        }
+        const int rows = std::max(1, 16384 / std::max(1, w.h.nx));
+        for (int y = 0; y < w.h.ny; y += rows) chunks.push_back({j, y, std::min(w.h.ny, y + rows)});
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < chunks.size();) {
+            const auto &w = b->inits[chunks[k].job];
+            init_profile_rows(w.h, w.d, b->stage + w.off, chunks[k].ya, chunks[k].yb);
+        }
+    };
+    const int nthr = (int)std::min<size_t>(chunks.size(),
+                                           std::min(16u, std::max(1u, std::thread::hardware_concurrency())));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthr; t++) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+    cudaError_t e = cudaSuccess;
+    for (const auto &w : b->inits)
+        if (e == cudaSuccess) e = launch_init_from(w.h, b->d_cases + w.slot, w.d, b->stage_dev + w.off, b->stream);
+    b->inits.clear();
+    return e;
+}
+
+int admit_cases(itlbm_batch *b) {
     b->stage_used = 0;  // the previous round's initial states are complete (advance ends synchronised)
     while (!b->pending.empty() && !b->free_slots.empty()) {
         const Pending &p = b->pending.front();
@@ -300,10 +350,11 @@ int admit(itlbm_batch *b) {
         e = cudaMemcpyAsync(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream);
         if (p.snapshot.empty()) {
             const size_t len = profile_len(h, d);
+            // a full staging buffer is reused only after the profiles queued in it are launched
+            if (e == cudaSuccess && b->stage_used + len > b->stage_cap) e = flush_inits(b);
             if (e == cudaSuccess) e = stage_reserve(b, len);
             if (e == cudaSuccess) {
-                init_profile(h, d, b->stage + b->stage_used);
-                e = launch_init_from(h, b->d_cases + slot, d, b->stage_dev + b->stage_used, b->stream);
+                b->inits.push_back(itlbm_batch::InitJob{slot, d, h, b->stage_used});
                 b->stage_used += len;
             }
             if (e != cudaSuccess) return cuda_fail(e, "admission");
@@ -319,6 +370,13 @@ int admit(itlbm_batch *b) {
         b->pending.pop_front();
     }
     return ITLBM_OK;
+}
+
+int admit(itlbm_batch *b) {
+    const int r = admit_cases(b);
+    const cudaError_t e = flush_inits(b);
+    if (r) return r;
+    return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "initial states");
 }
 
 }  // namespace

@@ -170,6 +170,7 @@ cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case
                         cudaStream_t s);  // single cases: stages the profile, waits
 size_t profile_len(const CaseDev &c, const itlbm_case_desc &d);
 void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof);  // host, profile_len values
+void init_profile_rows(const CaseDev &c, const itlbm_case_desc &d, double *prof, int ya, int yb);
 cudaError_t launch_init_from(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
                              const double *prof, cudaStream_t s);  // prof readable by the device
 // Export populations to FP64 AoS (reference layout).  which = 0: state of buffer `cur`;

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <thread>
 #include <vector>
 
@@ -177,40 +178,28 @@ size_t profile_len(const CaseDev &c, const itlbm_case_desc &d) {
 }
 
 // Host side of the initial profile: the expressions of Initial_conditions.cpp:66-86 (drop) and
-// Imm_INCL.cpp:310-324 (strip), evaluated with the host's libm like the reference does.
-void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof) {
-    const long long n = (long long)c.nx * c.ny;
+// Imm_INCL.cpp:310-324 (strip), evaluated with the host's libm like the reference does.  A drop's
+// profile is filled for rows [ya, yb); a strip's (one value per distance class) whole, for any range.
+void init_profile_rows(const CaseDev &c, const itlbm_case_desc &d, double *prof, int ya, int yb) {
     if (d.geometry == ITLBM_GEOM_DROP) {
         const double radius = d.radius > 0.0 ? d.radius : 0.25 * (double)d.nx;
         const double k_perfil = d.k_profile;
         const int x0 = c.nx / 2, y0 = c.ny / 2;
-        auto rows = [&](int ya, int yb) {
-            for (int y = ya; y < yb; y++)
-                for (int x = 0; x < c.nx; x++) {
-                    const double dx = (double)(x - x0), dy = (double)(y - y0), dz = 0.0;
-                    const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
-                    double phi;
-                    if (k_perfil > 0.0) {
-                        double arg = k_perfil * (r - radius);
-                        if (arg > 60.0) arg = 60.0;
-                        if (arg < -60.0) arg = -60.0;
-                        phi = 1.0 / (1.0 + std::exp(arg));
-                    } else {
-                        phi = (r < radius) ? 1.0 : 0.0;
-                    }
-                    prof[(size_t)y * c.nx + x] = phi;
+        for (int y = ya; y < yb; y++)
+            for (int x = 0; x < c.nx; x++) {
+                const double dx = (double)(x - x0), dy = (double)(y - y0), dz = 0.0;
+                const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+                double phi;
+                if (k_perfil > 0.0) {
+                    double arg = k_perfil * (r - radius);
+                    if (arg > 60.0) arg = 60.0;
+                    if (arg < -60.0) arg = -60.0;
+                    phi = 1.0 / (1.0 + std::exp(arg));
+                } else {
+                    phi = (r < radius) ? 1.0 : 0.0;
                 }
-        };
-        // every node is independent: large boxes are split by rows over host threads
-        const int nthr = n < (1 << 16) ? 1 : (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
-        if (nthr == 1) {
-            rows(0, c.ny);
-        } else {
-            std::vector<std::thread> pool;
-            for (int t = 0; t < nthr; t++)
-                pool.emplace_back(rows, (int)((long long)c.ny * t / nthr), (int)((long long)c.ny * (t + 1) / nthr));
-            for (auto &th : pool) th.join();
-        }
+                prof[(size_t)y * c.nx + x] = phi;
+            }
     } else {
         const int N = c.nx, p = d.p, q = d.q;
         const double m = std::sqrt((double)(p * p + q * q));
@@ -221,6 +210,23 @@ void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof) {
             prof[s2] = 1.0 / (1.0 + std::exp(-k * dred));
         }
     }
+}
+
+// The whole profile; a large drop's rows are split over host threads (every node is independent).
+void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof) {
+    const long long n = (long long)c.nx * c.ny;
+    const int nthr = (d.geometry != ITLBM_GEOM_DROP || n < (1 << 16))
+                         ? 1
+                         : (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (nthr == 1) {
+        init_profile_rows(c, d, prof, 0, c.ny);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; t++)
+        pool.emplace_back(init_profile_rows, std::cref(c), std::cref(d), prof, (int)((long long)c.ny * t / nthr),
+                          (int)((long long)c.ny * (t + 1) / nthr));
+    for (auto &th : pool) th.join();
 }
 
 // The initial state from a profile already in memory the device can read (device memory, or

@@ -19,6 +19,7 @@
 // Every wait on a copy is bounded (1 s); a CTA that gives up sets an error flag that the host reads
 // (ITLBM_E_TIMEOUT) and returns once its other copies have landed or timed out as well.
 #include "itlbm_site.cuh"
+#include "itlbm_tma.cuh"
 
 #include <cuda.h>
 
@@ -55,50 +56,10 @@ __device__ __forceinline__ int wrapm(int a, int n) {
     return r < 0 ? r + n : r;
 }
 
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ unsigned long long gtimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-// Bounded wait for the phase of parity `par` to complete: false after 1 s.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned par) {
-    const unsigned a = smem_u32(bar);
-    const unsigned long long t0 = gtimer();
-    for (unsigned it = 0;; ++it) {
-        unsigned done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(done)
-            : "r"(a), "r"(par)
-            : "memory");
-        if (done) return true;
-        if ((it & 63) == 63 && gtimer() - t0 > 1000000000ull) return false;
-    }
-}
-
 // One row: the 19 planes from `plane` of buffer `buf`, columns x .. x + 39 of row y.
 __device__ __forceinline__ void tma_row(const CUtensorMap *map, float *dst, int x, int y, int plane, int buf,
                                         unsigned long long *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(plane), "r"(buf), "r"(smem_u32(bar))
-        : "memory");
+    tma_load_4d(map, dst, x, y, plane, buf, bar);
 }
 
 struct Item {
@@ -355,7 +316,7 @@ __global__ void __launch_bounds__(MT, 3) k_march(const CaseDev *__restrict__ cas
         // prologue: the halo rows above, slab 0, then slabs 1 and 2 in flight
         if (threadIdx.x == 0) {
             // the map was written by the host before the launch; order this proxy's view after it
-            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&c.tmap) : "memory");
+            tensormap_acquire(&c.tmap);
             issue_slab(c, it, -1, sm);
             issue_slab(c, it, 0, sm);
         }
@@ -427,18 +388,26 @@ int march_error_take() {
 
 // The 4-D view {nx, ny, 38 planes, 2 buffers} of an FP32 state for the row copies of k_march:
 // boxes of 40 columns x 1 row x 19 planes; columns outside [0, nx) read as zeros.
-cudaError_t encode_state_map(CaseDev &h, void *mem, size_t per_buf) {
-    typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+namespace {
+typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                             const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                             CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeFn encode_fn() {
     static EncodeFn fn = nullptr;
     if (!fn) {
         cudaDriverEntryPointQueryResult q;
         void *p = nullptr;
         cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
-        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return cudaErrorNotSupported;
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return nullptr;
         fn = (EncodeFn)p;
     }
+    return fn;
+}
+}  // namespace
+
+cudaError_t encode_state_map(CaseDev &h, void *mem, size_t per_buf) {
+    const EncodeFn fn = encode_fn();
+    if (!fn) return cudaErrorNotSupported;
     const cuuint64_t dims[4] = {(cuuint64_t)h.nx, (cuuint64_t)h.ny, (cuuint64_t)(2 * NV), 2};
     const cuuint64_t strides[3] = {(cuuint64_t)h.pitch * 4, (cuuint64_t)h.stride * 4, (cuuint64_t)per_buf};
     const cuuint32_t box[4] = {(cuuint32_t)BW, 1, (cuuint32_t)NV, 1};
@@ -448,6 +417,5 @@ cudaError_t encode_state_map(CaseDev &h, void *mem, size_t per_buf) {
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
-
 
 }  // namespace itlbm

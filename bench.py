@@ -25,6 +25,7 @@ roofline algorithmic bytes per update: 38 populations read + 38 written (304 B i
         FP64) x nodes / mean kernel duration, against the measured copy bandwidth.
 fp64_one_at_a_time_mix  the plain FP64 path on the same mixed sweep, one case at a time (every
         10th case of the mix, 40 steps each): the denominator of the batched-vs-plain ratio.
+fp64_batched_mix  the same 600-case batch advanced by the batch engine in the plain FP64 path.
 latency the served stream (Poisson arrivals, scaled to a bench run) fed into one batch as requests
         arrive, at 70 % of the capacity the batch sustains on that stream (measured first with every
         request submitted at once): p50 / p99 time-to-result, wall clock.
@@ -572,6 +573,15 @@ def main():
             "workload": "4096x4096x1 static drop R=400, P3 chi=0.5, FP64 plain (bit-identical to the reference)"}
 
     fp64_mix = fp64_one_at_a_time(pkg) if args.workload == "batch600" else None
+    # the same 600-case batch in the plain FP64 path (bit-identical to the reference): what batching
+    # alone gains over one case at a time, at the reference's precision
+    fp64_batch = None
+    if args.workload == "batch600":
+        kb = min(args.steps, 100)
+        nb64, msb64, _, ncb64 = batch_run(pkg, kb, args.warmup, world, False, local, prec=pkg.PREC_F64)
+        fp64_batch = {"value": replica_mlups(nb64 * kb, msb64, world)[0], "unit": "MLUPS", "steps": kb,
+                      "cases": ncb64, "roofline_frac": 608.0 * nb64 * kb / (msb64 * 1e-3) / 1e9 / peak,
+                      "workload": "batch600 in the plain FP64 path (bit-identical to the reference)"}
     # the in-plane fold (nine classes per colour, 144 B per update): a separate variant, not the
     # headline D3Q19 number
     fold = None
@@ -611,6 +621,7 @@ def main():
             "fp32_single_4096": single32,
             "fp64_plain": fp64,
             "fp64_one_at_a_time_mix": fp64_mix,
+            "fp64_batched_mix": fp64_batch,
             "fold_variant": fold,
             "batched_fp32_over_plain_fp64": mlups / fp64["value"],
             "batched_fp32_over_fp64_one_at_a_time_mix": (mlups / fp64_mix["value"]) if fp64_mix else None,

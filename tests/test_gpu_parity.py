@@ -308,9 +308,11 @@ def test_fp32_tracks_fp64(gpu, name, tipo, chi, xi, A):
 def test_invalid_descriptions_are_rejected(itlbm):
     """Argument checks happen before any device work (no GPU needed, kept here with the case API)."""
     op = itlbm.make_op(3, 0.5)
-    for kw in ({"nx": 0}, {"tau": 0.0}, {"precision": 7}, {"geometry": 5}):
-        d = itlbm.desc(kw.get("nx", 16), 16, op, tau=kw.get("tau", 1.0), precision=kw.get("precision", 0),
-                       geometry=kw.get("geometry", 0))
+    # the last two: more than 2^30 nodes, and more tile rows than a work-table entry can address
+    for kw in ({"nx": 0}, {"tau": 0.0}, {"precision": 7}, {"geometry": 5}, {"nx": 40000, "ny": 40000},
+               {"nx": 1, "ny": 600000}):
+        d = itlbm.desc(kw.get("nx", 16), kw.get("ny", 16), op, tau=kw.get("tau", 1.0),
+                       precision=kw.get("precision", 0), geometry=kw.get("geometry", 0))
         with pytest.raises(itlbm.ItlbmError) as e:
             itlbm.Case(d)
         assert e.value.code == -1

@@ -65,7 +65,7 @@ PEAKS = REPO / "MEASURED_PEAKS.json"
 # HBM traffic per node of one FP32 step launch, dram__bytes_read.sum + dram__bytes_write.sum from one
 # ncu capture each: a launch over the 600-case batch (12.41 GB for 39 127 049 nodes) and a launch over
 # the 4096^2 drop (5.07 GB for 16 777 216 nodes).
-TRAFFIC_B_PER_NODE = {"batch600": 12406374400 / 39127049, "single": 5069217280 / 16777216}
+TRAFFIC_B_PER_NODE = {"batch600": 12406304768 / 39127049, "single": 5069217280 / 16777216}
 HBM_FALLBACK = 6650.0
 
 

@@ -138,6 +138,8 @@ def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600, prec
     upd = st1.node_updates - st0.node_updates
     assert upd % steps == 0 and st1.active == st0.active
     b.close()
+    global LAST_LAUNCH_MODE
+    LAST_LAUNCH_MODE = st1.launch_mode
     return upd // steps, ms, (sampler.summary() if sampler else None), st1.active
 
 
@@ -474,6 +476,9 @@ METRIC = "MLUPS & % HBM roofline, batched FP32 vs plain FP64 on 1 B200; p99 case
 REF_SAMPLE = 8  # cases of the batch mix the reference arm steps
 
 
+LAST_LAUNCH_MODE = None  # launch shape the batch engine's autotuner chose in the last batch_run
+
+
 def batch_config(nodes, ncases, world):
     return {"workload": "batch600: 600 cases (seed 20261203), side 64-512 log-uniform, 80% drops / 20% "
                         "inclined strips, 7 operators, tau 0.51-2, sigma 0.1-2, FP32 shifted storage",
@@ -549,10 +554,12 @@ def main():
     single = WORKLOADS["drop4096" if args.workload == "batch600" else args.workload]
     if args.workload == "batch600":
         nodes, ms, clocks, ncases = batch_run(pkg, args.steps, args.warmup, world, rank == 0, local)
+        mode = LAST_LAUNCH_MODE
         mlups, ms_max = replica_mlups(nodes * args.steps, ms, world)
         achieved = 304.0 * nodes * args.steps / (ms * 1e-3) / 1e9
         launches = args.steps  # one FP32 launch per step; the FP64 table is empty, so nothing is launched for it
         cfg = batch_config(nodes, ncases, world)
+        cfg["launch_shape"] = {-1: "one CTA per tile (autotuned)", 0: "persistent CTAs (autotuned)"}.get(mode, mode)
     else:
         nodes, ms, clocks = device_run(pkg, single, pkg.PREC_F32, args.steps, args.warmup, world,
                                        rank == 0, local)

@@ -226,7 +226,10 @@ typedef struct itlbm_batch_config {
     int    max_cases;         /* slots; 0 = 4096                                                  */
     int    chunk;             /* steps per graph replay; 0 = 500 (PASSOS_DIAG)                    */
     int    diag_every;        /* diagnostic interval; 0 = 500                                     */
-    int    ctas_per_sm;       /* 0 = one CTA per tile; > 0 = that many persistent CTAs per SM      */
+    int    ctas_per_sm;       /* launch shape of the step kernels: < 0 = one CTA per tile of the   */
+                              /* work table; > 0 = that many persistent CTAs per SM striding over */
+                              /* it; 0 = autotune: the first full replay times the two (persistent */
+                              /* at the occupancy limit) and keeps the faster (same results)       */
 } itlbm_batch_config;
 
 enum { ITLBM_EV_DIAG = 0, ITLBM_EV_DONE = 1, ITLBM_EV_UNSTABLE = 2 };
@@ -252,6 +255,8 @@ typedef struct itlbm_batch_stats {
     double    advance_ms;     /* host wall time spent inside itlbm_batch_advance                   */
     double    admit_ms;       /* of which admission: allocation and initial state of new cases     */
     double    capture_ms;     /* of which graph capture and instantiation                          */
+    int       launch_mode;    /* launch shape in use: -1 one CTA per tile, 0 persistent CTAs at   */
+                              /* the occupancy limit, k > 0 k persistent CTAs per SM               */
 } itlbm_batch_stats;
 
 /* No case memory is allocated until cases are admitted. */

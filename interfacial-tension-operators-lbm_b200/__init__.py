@@ -111,7 +111,8 @@ class BatchStats(C.Structure):
     _fields_ = [("active", C.c_int), ("pending", C.c_int), ("finished", C.c_int),
                 ("node_updates", C.c_longlong), ("device_ms", C.c_double), ("hbm_used", C.c_size_t),
                 ("replays", C.c_int), ("captures", C.c_int), ("diag_ms", C.c_double),
-                ("advance_ms", C.c_double), ("admit_ms", C.c_double), ("capture_ms", C.c_double)]
+                ("advance_ms", C.c_double), ("admit_ms", C.c_double), ("capture_ms", C.c_double),
+                ("launch_mode", C.c_int)]
 
 
 class ItlbmError(RuntimeError):

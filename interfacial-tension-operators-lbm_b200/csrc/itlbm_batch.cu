@@ -106,6 +106,13 @@ struct itlbm_batch {
     int *d_ntiles = nullptr;
     bool tables_dirty = true;
     int grid[NTAB] = {};
+    int ntab[NTAB] = {};  // current table lengths
+    int occ[NTAB] = {};   // resident CTAs per SM of each table's step kernel
+    // launch shape: -1 = one CTA per table entry, 0 = persistent CTAs at the occupancy limit, k > 0 =
+    // k persistent CTAs per SM; with ctas_per_sm = 0 the first full replay times -1 against 0
+    int mode = -1;
+    bool tuning = false;
+    cudaEvent_t tev[2] = {};
     bool march = false;  // FP32 cases run the marching kernel
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -144,6 +151,16 @@ int grid_bucket(int n) {
     return ((n + (1 << e) - 1) >> e) << e;
 }
 
+// Grids of the current launch shape: empty tables launch nothing; one CTA per entry rounds the
+// table up to its bucket; persistent CTAs stride over the table.
+void set_grids(itlbm_batch *b) {
+    for (int p = 0; p < NTAB; p++) {
+        if (b->ntab[p] == 0) b->grid[p] = 0;
+        else if (b->mode < 0) b->grid[p] = grid_bucket(b->ntab[p]);
+        else b->grid[p] = (b->mode > 0 ? b->mode : std::max(1, b->occ[p])) * b->sms;
+    }
+}
+
 int upload_tables(itlbm_batch *b) {
     std::vector<TileRef> t[NTAB];
     for (Active *a : b->slots) {
@@ -168,23 +185,23 @@ int upload_tables(itlbm_batch *b) {
             if (e != cudaSuccess) return cuda_fail(e, "work table upload");
         }
     }
-    if (b->cfg.ctas_per_sm <= 0)
-        for (int p = 0; p < NTAB; p++) b->grid[p] = grid_bucket(n[p]);
+    for (int p = 0; p < NTAB; p++) b->ntab[p] = n[p];
+    set_grids(b);
     // the graph reads the table pointers it was captured with: keep them, or re-capture
     cudaError_t e = cudaMemcpyAsync(b->d_ntiles, n, sizeof(int) * NTAB, cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "work table length");
     return cudaStreamSynchronize(b->stream) == cudaSuccess ? ITLBM_OK : cuda_fail(cudaGetLastError(), "sync");
 }
 
-// K sub-steps of every table on the batch stream: one table runs in line, several run as parallel
-// chains (fork, one chain per table on its own stream, join), in a capture or directly.
-cudaError_t enqueue_steps(itlbm_batch *b, int K) {
+// Sub-steps [k0, k1) of every table on the batch stream: one table runs in line, several run as
+// parallel chains (fork, one chain per table on its own stream, join), in a capture or directly.
+cudaError_t enqueue_steps(itlbm_batch *b, int k0, int k1) {
     int used = 0;
     for (int p = 0; p < NTAB; p++) used += b->grid[p] > 0;
     cudaError_t e = cudaSuccess;
     if (used <= 1) {
         for (int p = 0; p < NTAB; p++)
-            for (int k = 0; k < K && b->grid[p] > 0 && e == cudaSuccess; k++)
+            for (int k = k0; k < k1 && b->grid[p] > 0 && e == cudaSuccess; k++)
                 e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
                                 prec_of_table(p), p == 1 && b->march, b->stream);
         return e;
@@ -193,7 +210,7 @@ cudaError_t enqueue_steps(itlbm_batch *b, int K) {
     for (int p = 0; p < NTAB; p++) {
         if (b->grid[p] <= 0) continue;
         if ((e = cudaStreamWaitEvent(b->side[p], b->ev_fork, 0)) != cudaSuccess) return e;
-        for (int k = 0; k < K && e == cudaSuccess; k++)
+        for (int k = k0; k < k1 && e == cudaSuccess; k++)
             e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
                             prec_of_table(p), p == 1 && b->march, b->side[p]);
         if (e != cudaSuccess) return e;
@@ -222,7 +239,7 @@ int capture_graph(itlbm_batch *b) {
     cudaGraph_t g;
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "begin capture");
-    const cudaError_t el = enqueue_steps(b, b->cfg.chunk);
+    const cudaError_t el = enqueue_steps(b, 0, b->cfg.chunk);
     e = cudaStreamEndCapture(b->stream, &g);
     if (el != cudaSuccess) {
         if (e == cudaSuccess) cudaGraphDestroy(g);
@@ -232,6 +249,43 @@ int capture_graph(itlbm_batch *b) {
     e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
     return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "graph instantiate");
+}
+
+// Node updates of sub-steps [k0, k1) of this replay.
+long long updates_in(const itlbm_batch *b, int k0, int k1) {
+    long long u = 0;
+    for (const Active *a : b->slots)
+        if (a) u += (long long)std::max(0, std::min(a->chunk_len, k1) - k0) * a->desc.nx * a->desc.ny;
+    return u;
+}
+
+// Autotuning of the launch shape on the first full replay: sub-steps [0, M) with one CTA per table
+// entry, [M, 2M) with persistent CTAs at the occupancy limit, both timed with events; the faster
+// (per node update) runs the rest of the replay and is captured into the graph.  Both shapes run the
+// same kernel on the same tiles, so the results do not depend on the choice.
+int tune_and_run(itlbm_batch *b, int K) {
+    const int M = std::max(2, K / 8);
+    const int modes[2] = {-1, 0};
+    double rate[2] = {0, 0};
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < 2 && e == cudaSuccess; c++) {
+        b->mode = modes[c];
+        set_grids(b);
+        cudaEventRecord(b->tev[0], b->stream);
+        e = enqueue_steps(b, c * M, (c + 1) * M);
+        cudaEventRecord(b->tev[1], b->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b->tev[1]);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->tev[0], b->tev[1]);
+        rate[c] = ms > 0 ? (double)updates_in(b, c * M, (c + 1) * M) / ms : 0.0;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "launch-shape tuning");
+    // persistent CTAs only when clearly faster (the two are within noise on small tables)
+    b->mode = rate[1] > 1.02 * rate[0] ? 0 : -1;
+    b->tuning = false;
+    set_grids(b);
+    if ((e = enqueue_steps(b, 2 * M, K)) != cudaSuccess) return cuda_fail(e, "step launches");
+    return capture_graph(b);
 }
 
 void retire(itlbm_batch *b, Active *a) {
@@ -419,10 +473,13 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
         cuuint64_t keep = b->cfg.hbm_budget;
         cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
-    // launch shape: one CTA per tile of the work table (the grid follows the table and the graph is
-    // re-captured when it changes), or, with ctas_per_sm > 0, that many persistent CTAs per SM
-    // striding over the table
-    for (int p = 0; p < NTAB; p++) b->grid[p] = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm * b->sms : 0;
+    // launch shape: ctas_per_sm < 0, one CTA per entry of the work table (the grid follows the table
+    // and the graph is re-captured when it changes); > 0, that many persistent CTAs per SM striding
+    // over it; 0, whichever of the two (persistent at the occupancy limit) the first full replay
+    // measures faster
+    b->mode = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm : -1;
+    b->tuning = b->cfg.ctas_per_sm == 0;
+    for (int p = 0; p < NTAB; p++) b->occ[p] = step_occupancy(prec_of_table(p));
     const int M = b->cfg.max_cases;
     b->slots.assign(M, nullptr);
     for (int s = M - 1; s >= 0; s--) b->free_slots.push_back(s);
@@ -451,6 +508,7 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
     cudaEventCreate(&b->ev0);
     cudaEventCreate(&b->ev1);
     cudaEventCreate(&b->ev2);
+    for (int t = 0; t < 2; t++) cudaEventCreate(&b->tev[t]);
     if ((e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess) {
         itlbm_batch_destroy(b);
         return cuda_fail(e, "batch events");
@@ -494,6 +552,8 @@ void itlbm_batch_destroy(itlbm_batch *b) {
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->ev2) cudaEventDestroy(b->ev2);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (int t = 0; t < 2; t++)
+        if (b->tev[t]) cudaEventDestroy(b->tev[t]);
     for (int p = 0; p < NTAB; p++) {
         if (b->ev_join[p]) cudaEventDestroy(b->ev_join[p]);
         if (b->side[p]) cudaStreamDestroy(b->side[p]);
@@ -595,11 +655,14 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         b->tables_dirty = false;
     }
     cudaEventRecord(b->ev0, b->stream);
-    if (K == b->cfg.chunk) {
+    if (b->tuning && K == b->cfg.chunk && K >= 16) {
+        r = tune_and_run(b, K);
+        if (r) return r;
+    } else if (K == b->cfg.chunk) {
         e = cudaGraphLaunch(b->graph, b->stream);
         if (e != cudaSuccess) return cuda_fail(e, "graph launch");
     } else {
-        if ((e = enqueue_steps(b, K)) != cudaSuccess) return cuda_fail(e, "step launches");
+        if ((e = enqueue_steps(b, 0, K)) != cudaSuccess) return cuda_fail(e, "step launches");
     }
     cudaEventRecord(b->ev1, b->stream);
     b->replays++;
@@ -718,6 +781,7 @@ int itlbm_batch_stats_get(const itlbm_batch *b, itlbm_batch_stats *out) {
     out->advance_ms = b->advance_ms;
     out->admit_ms = b->admit_ms;
     out->capture_ms = b->capture_ms;
+    out->launch_mode = b->mode;
     return ITLBM_OK;
 }
 

@@ -356,7 +356,8 @@ int main(int argc, char **argv) {
            << ", \"mlups_device\": " << (st.device_ms > 0 ? st.node_updates / (st.device_ms * 1e3) : 0.0)
            << ", \"diag_ms\": " << st.diag_ms << ", \"advance_ms\": " << st.advance_ms
            << ", \"admit_ms\": " << st.admit_ms << ", \"capture_ms\": " << st.capture_ms
-           << ", \"captures\": " << st.captures << ", \"hbm_used\": " << st.hbm_used << "}\n";
+           << ", \"captures\": " << st.captures << ", \"launch_mode\": " << st.launch_mode
+           << ", \"hbm_used\": " << st.hbm_used << "}\n";
         std::string stats = js.str();
         for (size_t pos; (pos = stats.find("nan")) != std::string::npos;) stats.replace(pos, 3, "null");
         write_text(join(spool, "serve_stats.json"), stats);

@@ -139,3 +139,30 @@ def test_many_cases_start_clean(gpu):
             alone = c.diag_drop(0).as_dict()
         for key in ("massa_R", "massa_B", "u_max", "raio", "delta_p", "min_f"):
             assert alone[key] == rows[k][key] or abs(alone[key] - rows[k][key]) <= 1e-12 * abs(alone[key]) + 1e-15, (k, key)
+
+
+def test_launch_shapes_agree(gpu):
+    """The autotuned batch (ctas_per_sm = 0), one CTA per tile (-1) and persistent CTAs (4 per SM) run
+    the same kernels on the same tiles: the same bits.  The tuned batch reports the shape it chose."""
+    cases = [(48, 3, 0.5, 0.225, 1, 0, (1, 0)), (40, 12, 0.5, 0.1, 0, 0, (1, 0)),
+             (56, 11, 0.5, 0.1, 2, 1, (2, 1)), (37, 13, 0.5, 0.1, 1, 0, (1, 0))]
+    descs = [mkdesc(gpu, nx, t, chi, A=A, prec=pr, geometry=g, p=pq[0], q=pq[1])
+             for nx, t, chi, A, pr, g, pq in cases]
+    rows, modes = {}, {}
+    for cps in (0, -1, 4):
+        with gpu.Batch(chunk=64, ctas_per_sm=cps) as b:
+            for k, d in enumerate(descs):
+                b.submit(d, 129, k)
+            events = []
+            for _ in range(20):
+                b.advance()
+                events += b.poll()
+                st = b.stats()
+                if st.active == 0 and st.pending == 0:
+                    break
+            modes[cps] = st.launch_mode
+        rows[cps] = [(e.tag, e.step, (e.drop if cases[e.tag][5] == 0 else e.strip).as_dict())
+                     for e in events if e.kind == gpu.EV_DIAG]
+    assert len(rows[0]) == 2 * len(cases)  # the diagnostics at steps 0 and 128
+    assert rows[0] == rows[-1] == rows[4]
+    assert modes[-1] == -1 and modes[4] == 4 and modes[0] in (-1, 0)

@@ -260,11 +260,11 @@ long long updates_in(const itlbm_batch *b, int k0, int k1) {
 }
 
 // Autotuning of the launch shape on the first full replay: sub-steps [0, M) with one CTA per table
-// entry, [M, 2M) with persistent CTAs at the occupancy limit, both timed with events; the faster
+// entry (M = K / 16), [M, 2M) with persistent CTAs at the occupancy limit, both timed with events; the faster
 // (per node update) runs the rest of the replay and is captured into the graph.  Both shapes run the
 // same kernel on the same tiles, so the results do not depend on the choice.
 int tune_and_run(itlbm_batch *b, int K) {
-    const int M = std::max(2, K / 8);
+    const int M = std::max(2, K / 16);
     const int modes[2] = {-1, 0};
     double rate[2] = {0, 0};
     cudaError_t e = cudaSuccess;

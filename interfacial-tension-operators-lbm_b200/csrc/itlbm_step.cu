@@ -83,12 +83,17 @@ __device__ __forceinline__ int wrap_near(int a, int n) {
     return r;
 }
 
+// Stride of the per-node auxiliary values in shared memory: 7, odd, so that the 32 lanes reading one
+// component of consecutive nodes hit distinct banks (a stride of 6 words, or 12 for doubles, puts two
+// lanes on each bank).
+constexpr int AUXS = 7;
+
 template <class S>
 struct SmemT {
     S phi[PY][PX];        // rho^N of tile + halo (HMAX), position (px, py) = global (x0-2+px, y0-2+py)
     S rsum[2][PY * PX - TX * TY];  // halo ring: the two colour sums of each ring node
     S g[QY][QX][3];       // ring-1 gradient (F1, F2)
-    S aux[QY][QX][6];     // ring-1 normal (F1) or stress (F2)
+    S aux[QY][QX][AUXS];  // ring-1 normal (F1) or stress (F2), 6 values at an odd stride
 };
 
 // rho^N from the two colour sums.  FP64: (rho_R - rho_B) / (rho_R + rho_B), Imm_OPS.cpp:255-258.
@@ -257,7 +262,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             if constexpr (std::is_same<S, float>::value)
                 kappa = curvature_plane([&](int dx, int dy) { return sm.aux[qy + dy][qx + dx]; });
             else
-                kappa = curvature<S, 6>(sm.aux, qx, qy);
+                kappa = curvature<S, AUXS>(sm.aux, qx, qy);
             const S hs = (S(0.5) * (S)c.sigma) * kappa;
             Fx = hs * sm.g[qy][qx][0];
             Fy = hs * sm.g[qy][qx][1];
@@ -266,7 +271,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             if constexpr (std::is_same<S, float>::value)
                 stress_div_plane([&](int dx, int dy) { return sm.aux[ly + 1 + dy][lx + 1 + dx]; }, Fx, Fy);
             else
-                stress_div<S, 6>(sm.aux, lx + 1, ly + 1, Fx, Fy, Fz);
+                stress_div<S, AUXS>(sm.aux, lx + 1, ly + 1, Fx, Fy, Fz);
         } else if (tipo == ITLBM_OP_F3) {
             S g0, g1, g2, mu;
             if constexpr (std::is_same<S, float>::value) {

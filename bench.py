@@ -118,7 +118,10 @@ def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600, prec
     # reference would stop it), so the timed node count is that of the cases still running
     assert st.active + st.finished == n_cases, f"only {st.active + st.finished} of {n_cases} cases admitted"
     b.poll()
-    b.advance()  # warm-up replay
+    # warm-up: at least `warmup` steps, in whole replays of the graph that is timed (the first full
+    # replay also runs the launch-shape autotuning)
+    for _ in range(max(1, -(-warmup // steps))):
+        b.advance()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
@@ -227,6 +230,118 @@ def served_latency(pkg, load=0.7):
                         "last step's diagnostic"}
 
 
+def c5_stream(seed=20261203, n=32):
+    """The served-stream configuration at its specified sizes: Poisson arrivals of cases with side
+    log-uniform in 64-2048 and 5 000-100 000 steps, 10 % FP64, 80 % drops / 20 % inclined strips,
+    operators, tau and sigma as in the batch mix; a bounded number of requests."""
+    import numpy as np
+    rng = np.random.default_rng(seed + 2)
+    ops = [(1, 0.5), (3, -0.4), (3, 0.5), (3, 2.0), (11, 0.5), (12, 0.5), (13, 0.5)]
+    reqs = []
+    for _ in range(n):
+        side = int(round(math.exp(rng.uniform(math.log(64), math.log(2048)))))
+        strip = rng.uniform() < 0.2
+        tipo, chi = ops[rng.integers(len(ops))]
+        tau = float(rng.uniform(0.51, 2.0))
+        sigma = float(math.exp(rng.uniform(math.log(0.1), math.log(2.0))))
+        A = 9.0 * sigma / (4.0 * tau) if tipo < 11 else sigma
+        p, q = (int(rng.integers(1, 5)), int(rng.integers(1, 5))) if strip else (1, 0)
+        radius = float(rng.uniform(10.0, side / 4.0)) if not strip else 0.0
+        reqs.append(dict(nx=side, tipo=tipo, chi=chi, tau=tau, A=A, strip=strip, p=p, q=q, radius=radius,
+                         steps=int(rng.integers(5000, 100001)), fp64=bool(rng.uniform() < 0.1)))
+    return reqs, rng.exponential(1.0, n)
+
+
+def fifo_latency(arrive, service, servers=1):
+    """Time-to-result of requests served first come, first served by `servers` identical servers."""
+    import heapq
+    free = [0.0] * servers
+    out = []
+    for a, s in zip(arrive, service):
+        t = heapq.heappop(free)
+        start = max(t, a)
+        heapq.heappush(free, start + s)
+        out.append(start + s - a)
+    return out
+
+
+def served_latency_c5(pkg, capacity_mlups, load=0.7, n=32):
+    """The specified served stream fed into one batch as requests arrive (offered load `load` of the
+    capacity the batch reaches on the 600-case mix), time-to-result from submission to the last step's
+    diagnostic; beside it, the same arrivals served one case at a time by the plain FP64 path (each
+    request's service time from its own CUDA-event-timed FP64 steps, queued first come, first served)."""
+    import numpy as np
+    import torch
+    reqs, gaps = c5_stream(n=n)
+    work = np.array([r["nx"] ** 2 * r["steps"] for r in reqs], dtype=float)
+    rate = load * capacity_mlups * 1e6 / work.mean()
+    arrive = np.cumsum(gaps / rate)
+    b = pkg.Batch(chunk=500, diag_every=500)
+    t0 = time.perf_counter()
+    nxt, lat, done = 0, [], 0
+    while done < len(reqs):
+        now = time.perf_counter() - t0
+        while nxt < len(reqs) and arrive[nxt] <= now:
+            r = reqs[nxt]
+            b.submit(batch_desc(pkg, r, pkg.PREC_F64 if r["fp64"] else pkg.PREC_F32), r["steps"], nxt)
+            nxt += 1
+        st = b.stats()
+        if st.active == 0 and st.pending == 0:
+            if nxt < len(reqs):
+                time.sleep(min(0.01, max(0.0, arrive[nxt] - now)))
+            continue
+        b.advance()
+        for e in b.poll():
+            if e.kind != pkg.EV_DIAG:
+                lat.append(e.t_event - e.t_submit)
+                done += 1
+    wall = time.perf_counter() - t0
+    st = b.stats()
+    b.close()
+    # the plain FP64 path, one case at a time: each request's own rate over 100 timed steps
+    stream = torch.cuda.current_stream()
+    service = []
+    for r in reqs:
+        case = pkg.Case(batch_desc(pkg, r, pkg.PREC_F64))
+        case.step(3, stream=stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        case.step(100, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        service.append(e0.elapsed_time(e1) * 1e-3 * r["steps"] / 100.0)
+        case.close()
+    lat64 = np.array(fifo_latency(arrive, service))
+    lat = np.array(lat)
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "max_s": float(lat.max()), "requests": len(reqs), "offered_load": load,
+            "capacity_mlups": capacity_mlups, "achieved_mlups": st.node_updates / wall / 1e6, "wall_s": wall,
+            "node_updates": float(work.sum()), "diag_ms": st.diag_ms,
+            "fp64_one_at_a_time": {"p50_s": float(np.percentile(lat64, 50)),
+                                   "p99_s": float(np.percentile(lat64, 99)),
+                                   "mlups": float(work.sum() / sum(service) / 1e6),
+                                   "model": "same arrivals, one FP64 case at a time first come first served; "
+                                            "service time of each request from 100 CUDA-event-timed steps of "
+                                            "it alone, scaled to its step count"},
+            "workload": f"served stream at its specified sizes: {len(reqs)} Poisson arrivals, side 64-2048, "
+                        "5000-100000 steps, 10% FP64, 80% drops / 20% strips, 7 operators; offered load "
+                        "relative to the batch600 throughput; time-to-result from submission to the last "
+                        "step's diagnostic"}, reqs, arrive
+
+
+def c5_cpu_estimate(reqs, arrive, mlups_1thread, cores):
+    """The same requests on the reference's CPU path as rodar_lote.py runs it: one single-threaded
+    process per case, `cores` of them at a time, each at the measured one-thread rate of the
+    reference's step loop, first come first served (a model, not a run)."""
+    import numpy as np
+    service = [r["nx"] ** 2 * r["steps"] / (mlups_1thread * 1e6) for r in reqs]
+    lat = np.array(fifo_latency(arrive, service, servers=cores))
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "processes": cores, "mlups_per_process": mlups_1thread,
+            "model": "the same arrivals, one single-threaded reference process per case on each host core "
+                     "(rodar_lote.py's process pool), each at the measured one-thread rate"}
+
+
 def batch_e2e(pkg, steps, n_cases=600):
     """The batch through the C ABI, wall clock: submit every case, advance until each has run
     `steps` steps (diagnostics every 500 steps fall due on the way), poll the events."""
@@ -247,10 +362,14 @@ def batch_e2e(pkg, steps, n_cases=600):
     dt = time.perf_counter() - t0
     upd = st.node_updates
     b.close()
+    diag_rounds = -(-steps // 500)  # diagnostic rounds after step 0: every 500 steps and the last
     h2d = 8 * nodes
     d2h = nev * ctypes.sizeof(pkg.BatchEvent)
     return {"value": upd / dt / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": d2h / steps, "wall_s": dt, "events": nev,
+            "device_ms": st.device_ms, "diag_ms": st.diag_ms,
+            "diag_ms_per_500_steps": st.diag_ms / (diag_rounds + 1), "admit_ms": st.admit_ms,
+            "capture_ms": st.capture_ms, "advance_ms": st.advance_ms,
             "note": "whole batch through itlbm_batch_*: host profiles up, diagnostics down; unstable "
                     "cases retire early, so node updates are counted, not assumed"}
 
@@ -473,7 +592,7 @@ def cpu_baseline(threads=0):
 
 
 METRIC = "MLUPS & % HBM roofline, batched FP32 vs plain FP64 on 1 B200; p99 case latency"
-REF_SAMPLE = 8  # cases of the batch mix the reference arm steps
+REF_EVERY = 10  # the reference arm steps every 10th case of the batch mix (60 cases spread over it)
 
 
 LAST_LAUNCH_MODE = None  # launch shape the batch engine's autotuner chose in the last batch_run
@@ -488,31 +607,61 @@ def batch_config(nodes, ncases, world):
 
 def run_reference(args):
     """The reference's own CPU step loop on the host cores, same metric and workload, rank 0 only.
-    Each step is one step of each of the first REF_SAMPLE cases of the batch mix (the reference runs
-    one case per process; a strip steps like a drop of its size and operator -- the step loop does
-    not depend on the initial state)."""
+    Each step is one step of each case of a sample spread over the batch mix (every REF_EVERY-th case):
+    drops through the Imm_OPS step loop, inclined strips through the Imm_INCL one.  The cases run the
+    way the reference runs a batch (rodar_lote.py's pool: one single-threaded run per case, as many at
+    a time as there are cores): one host thread per core, each stepping its share of the cases with
+    one OpenMP thread, largest cases first; the time is the wall clock of the whole sample."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    os.environ["OMP_NUM_THREADS"] = "1"  # before the reference's OpenMP runtime is loaded
+    import concurrent.futures
     import oracle
     if args.workload == "batch600":
         mix = batch_mix()
-        sample = [dict(nx=c["nx"], ny=c["nx"], tipo=c["tipo"], chi=c["chi"], tau=c["tau"], A=c["A"],
-                       radius=c["radius"]) for c in mix[:REF_SAMPLE]]
+        sample = mix[::REF_EVERY]
         cfg = batch_config(sum(c["nx"] * c["nx"] for c in mix), len(mix), args.gpus)
-        desc = f"first {REF_SAMPLE} cases of the batch mix, sides " + ",".join(str(c["nx"]) for c in sample)
+        names = {1: "P1", 3: "P3", 11: "F1", 12: "F2", 13: "F3"}
+        ops = {}
+        for c in sample:
+            k = names[c["tipo"]] + (f" chi={c['chi']}" if c["tipo"] == 3 else "")
+            ops[k] = ops.get(k, 0) + 1
+        nstrip = sum(1 for c in sample if c["strip"])
+        desc = (f"every {REF_EVERY}th case of the batch mix: {len(sample)} cases, "
+                f"{sum(c['nx'] ** 2 for c in sample)} nodes, {len(sample) - nstrip} drops / {nstrip} strips, "
+                f"sides {min(c['nx'] for c in sample)}-{max(c['nx'] for c in sample)}, operators "
+                + ", ".join(f"{k} x{v}" for k, v in sorted(ops.items())))
     else:
         w = WORKLOADS[args.workload]
-        sample = [dict(nx=1024, ny=1024, tipo=w["tipo"], chi=w["chi"], tau=w["tau"], A=w["A"], radius=100.0)]
+        sample = [dict(nx=1024, tipo=w["tipo"], chi=w["chi"], tau=w["tau"], A=w["A"], radius=100.0, strip=False)]
         cfg = {"workload": args.workload, "nodes": w["nx"] * w["ny"], "parallelism": f"replicas x{args.gpus}"}
         desc = f"1024x1024 sample of {args.workload}"
-    steppers = [oracle.RefStepper(c["nx"], c["ny"], c["tipo"], c["chi"], 1.569988, c["tau"], 0.8, c["A"],
-                                  c["radius"]) for c in sample]
-    for r in steppers:
-        r.step(args.warmup)
-    dt = sum(r.step(args.steps) for r in steppers)
+    steppers = []
+    for c in sample:
+        if c["strip"]:
+            steppers.append(oracle.RefStripStepper(c["nx"], c["tipo"], c["p"], c["q"], c["chi"], 1.569988,
+                                                   c["tau"], 0.8, c["A"], threads=1))
+        else:
+            steppers.append(oracle.RefStepper(c["nx"], c["nx"], c["tipo"], c["chi"], 1.569988, c["tau"], 0.8,
+                                              c["A"], c["radius"], threads=1))
+    nthr = min(os.cpu_count() or 1, len(steppers))
+    shares = [[] for _ in range(nthr)]
+    load = [0] * nthr
+    for r in sorted(steppers, key=lambda r: -r.nodes):  # largest first onto the least loaded thread
+        k = load.index(min(load))
+        shares[k].append(r)
+        load[k] += r.nodes
+
+    def run_all(n):
+        with concurrent.futures.ThreadPoolExecutor(nthr) as ex:  # the steps release the interpreter lock
+            list(ex.map(lambda sh: [r.step(n) for r in sh], shares))
+
+    run_all(args.warmup)
+    t0 = time.perf_counter()
+    run_all(args.steps)
+    dt = time.perf_counter() - t0
     upd = sum(r.nodes for r in steppers) * args.steps
-    nthr = steppers[0].threads
     for r in steppers:
         r.close()
     mlups = upd / dt / 1e6
@@ -522,8 +671,10 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": nthr, "kind": "reference",
-                             "sample": f"{desc}; {args.steps} steps each, reference step loop "
-                                       f"(Imm_OPS.cpp:252-287, oracle/_ref, its own flags), {nthr} OpenMP threads"},
+                             "sample": f"{desc}; {args.steps} steps each, the reference's step loops "
+                                       f"(Imm_OPS.cpp:252-287, Imm_INCL.cpp:364-396; oracle/_ref, its own "
+                                       f"flags), one single-threaded case at a time per host thread, "
+                                       f"{nthr} threads"},
             "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -539,6 +690,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-latency", action="store_true")
+    ap.add_argument("--c5-requests", type=int, default=32, help="requests of the specified served stream (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -608,12 +760,17 @@ def main():
         e2e = batch_e2e(pkg, 1001) if args.workload == "batch600" else e2e_run(pkg, single, pkg.PREC_F32, args.steps)
         if world > 1:
             e2e["value"] = allreduce_sum(e2e["value"], world)
-    latency = None
+    latency = latency_c5 = None
     if not args.no_latency and args.workload == "batch600":
         latency = served_latency(pkg)
+        if args.c5_requests > 0:
+            latency_c5, c5_reqs, c5_arrive = served_latency_c5(pkg, mlups / world, n=args.c5_requests)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
+        if latency_c5 is not None and cpu is not None:
+            latency_c5["reference_cpu"] = c5_cpu_estimate(c5_reqs, c5_arrive, cpu["single_thread"]["value"],
+                                                          cpu["host"]["logical_cores"])
 
     if rank == 0:
         line = {
@@ -624,7 +781,10 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_lu": 304.0,
                          "traffic": TRAFFIC_B_PER_NODE["batch600" if args.workload == "batch600" else "single"] * nodes,
-                         "traffic_note": "bytes per launch, from one ncu capture, scaled by nodes per launch"},
+                         "traffic_note": "bytes per launch: dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                         "ncu capture (profiles/k_step_f32_batch600_traffic.md, "
+                                         "profiles/k_step_f32_drop4096_traffic.md), per node, times the "
+                                         "nodes of one launch"},
             "fp32_single_4096": single32,
             "fp64_plain": fp64,
             "fp64_one_at_a_time_mix": fp64_mix,
@@ -636,6 +796,7 @@ def main():
             "clocks": clocks,
             "e2e": e2e,
             "latency": latency,
+            "latency_c5": latency_c5,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

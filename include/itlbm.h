@@ -194,12 +194,25 @@ int  itlbm_case_read_pops(itlbm_case *c, int which, double *fR, double *fB);
 /* Sync.  Overwrites the state at the top of the next step (same layout as read_pops which = 0). */
 int  itlbm_case_write_pops(itlbm_case *c, const double *fR, const double *fB);
 
+/* The two forms of the per-node velocity that the reference's output files carry. */
+enum {
+    ITLBM_FIELDS_VTK = 0,     /* vel_*.vtk, rec_velocity (LBM_functions.cpp:1349-1458): the colour    */
+                              /* velocities of calcula weighted by the concentrations, u = c_R u_R +  */
+                              /* c_B u_B, minus (F/2)/rho for a case with a force                       */
+    ITLBM_FIELDS_PROFILE = 1  /* perfil.dat, mede_inclinada (Imm_INCL.cpp:104-162): the mixture       */
+                              /* momentum, u = (sum_i f_i c_i - F/2) / rho (NaN where !(rho > 0))      */
+};
+
 /* Sync.  Per-node fields of the post-collision populations of the last step, each nx*ny doubles in
- * pto order (any pointer may be NULL): rho_R and rho_B (rec_density, LBM_functions.cpp:1462-1511),
- * the mixture velocity with the Guo half-force removed (rec_velocity, LBM_functions.cpp:1349-1458),
- * and the force of the last step (`forca`, Imm_OPS.cpp:174-181), 3 per node. */
+ * pto order (any pointer may be NULL): rho_R and rho_B (rec_density, LBM_functions.cpp:1457-1511),
+ * the velocity of vel_*.vtk (ITLBM_FIELDS_VTK: rec_velocity, LBM_functions.cpp:1349-1458, the Guo
+ * half-force removed) and the force of the last step (`forca`, Imm_OPS.cpp:174-181), 3 per node.
+ * In FP64 every value is the reference's, rounded as the reference rounds it. */
 int  itlbm_case_read_fields(itlbm_case *c, double *rho_R, double *rho_B, double *ux, double *uy,
                             double *uz, double *force);
+/* Sync.  The per-node values perfil.dat prints (Imm_INCL.cpp:101-162): rho_R, rho_B and the
+ * ITLBM_FIELDS_PROFILE velocity (ux, uy), post-collision populations of the last step. */
+int  itlbm_case_read_profile(itlbm_case *c, double *rho_R, double *rho_B, double *ux, double *uy);
 
 /* Sync.  Case snapshots: the reference restarts an interrupted batch from step 0 (rodar_lote.py:5-7);
  * these save a case (its description, its step count and its populations at the top of its next
@@ -257,6 +270,7 @@ typedef struct itlbm_batch_stats {
     double    capture_ms;     /* of which graph capture and instantiation                          */
     int       launch_mode;    /* launch shape in use: -1 one CTA per tile, 0 persistent CTAs at   */
                               /* the occupancy limit, k > 0 k persistent CTAs per SM               */
+    int       held;           /* finished cases kept for itlbm_batch_read_fields (not in `active`) */
 } itlbm_batch_stats;
 
 /* No case memory is allocated until cases are admitted. */
@@ -278,6 +292,19 @@ int  itlbm_batch_advance(itlbm_batch *b, void *stream);
 /* Copies up to `max` waiting events (oldest first) and removes them from the queue. */
 int  itlbm_batch_poll(itlbm_batch *b, itlbm_batch_event *ev, int max);
 int  itlbm_batch_stats_get(const itlbm_batch *b, itlbm_batch_stats *out);
+
+/* Final fields of batch cases (the files Imm_OPS.cpp:357-364 and Imm_INCL.cpp:101-162 write at the
+ * last step).  With itlbm_batch_hold_finished(b, 1), a case that retires (ITLBM_EV_DONE, or
+ * ITLBM_EV_UNSTABLE) keeps its state on the device, off the work table and still counted against
+ * the HBM budget, until itlbm_batch_release; itlbm_batch_read_fields reads the post-collision fields
+ * of its last measured step in the given ITLBM_FIELDS_* form (same values as itlbm_case_read_fields /
+ * itlbm_case_read_profile; any pointer may be NULL).  read_fields also accepts an active case whose
+ * last advance ended at one of its diagnostic steps.  ITLBM_E_ARG for an unknown tag, ITLBM_E_STATE
+ * when the case has no measured step to read. */
+int  itlbm_batch_hold_finished(itlbm_batch *b, int on);
+int  itlbm_batch_read_fields(itlbm_batch *b, long long tag, int form, double *rho_R, double *rho_B,
+                             double *ux, double *uy, double *uz);
+int  itlbm_batch_release(itlbm_batch *b, long long tag);
 
 /* ---- operator seam on the device (per-site functions of the reference) -------------------- */
 /* Each call copies its host arrays to the device, runs the same device code the step kernel uses,

@@ -25,6 +25,7 @@ N_ANG = 256
 OP_P1, OP_P3, OP_F1, OP_F2, OP_F3 = 1, 3, 11, 12, 13
 GEOM_DROP, GEOM_STRIP = 0, 1
 PREC_F64, PREC_F32, PREC_F32_FOLD = 0, 1, 2
+FIELDS_VTK, FIELDS_PROFILE = 0, 1
 STEP_KEEP_AUX = 1
 
 ERRORS = {
@@ -112,7 +113,7 @@ class BatchStats(C.Structure):
                 ("node_updates", C.c_longlong), ("device_ms", C.c_double), ("hbm_used", C.c_size_t),
                 ("replays", C.c_int), ("captures", C.c_int), ("diag_ms", C.c_double),
                 ("advance_ms", C.c_double), ("admit_ms", C.c_double), ("capture_ms", C.c_double),
-                ("launch_mode", C.c_int)]
+                ("launch_mode", C.c_int), ("held", C.c_int)]
 
 
 class ItlbmError(RuntimeError):
@@ -152,6 +153,7 @@ def lib():
         "itlbm_case_read_pops": (C.c_int, [vp, C.c_int, dp, dp]),
         "itlbm_case_write_pops": (C.c_int, [vp, dp, dp]),
         "itlbm_case_read_fields": (C.c_int, [vp, dp, dp, dp, dp, dp, dp]),
+        "itlbm_case_read_profile": (C.c_int, [vp, dp, dp, dp, dp]),
         "itlbm_case_save": (C.c_int, [vp, C.c_char_p]),
         "itlbm_case_load": (C.c_int, [C.c_char_p, P(vp)]),
         "itlbm_snapshot_info": (C.c_int, [C.c_char_p, P(CaseDesc), P(C.c_longlong)]),
@@ -163,6 +165,9 @@ def lib():
         "itlbm_batch_advance": (C.c_int, [vp, vp]),
         "itlbm_batch_poll": (C.c_int, [vp, P(BatchEvent), C.c_int]),
         "itlbm_batch_stats_get": (C.c_int, [vp, P(BatchStats)]),
+        "itlbm_batch_hold_finished": (C.c_int, [vp, C.c_int]),
+        "itlbm_batch_read_fields": (C.c_int, [vp, C.c_longlong, C.c_int, dp, dp, dp, dp, dp]),
+        "itlbm_batch_release": (C.c_int, [vp, C.c_longlong]),
         "itlbm_dev_perturbacao": (C.c_int, [P(Operador), C.c_double, C.c_int, dp, dp]),
         "itlbm_dev_source": (C.c_int, [C.c_int, dp, dp, dp, C.c_double, dp]),
         "itlbm_dev_calcula_forca": (C.c_int, [P(Operador), C.c_double, C.c_int, C.c_int, dp, dp, dp]),
@@ -314,6 +319,14 @@ class Case:
             out["force"] = F
         return out
 
+    def read_profile(self):
+        """The per-node values of perfil.dat (rho_R, rho_B and the mixture velocity ux, uy)."""
+        n = self.n
+        out = {k: np.empty(n) for k in ("rho_R", "rho_B", "ux", "uy")}
+        check(lib().itlbm_case_read_profile(self._h, *[_dp(out[k]) for k in ("rho_R", "rho_B", "ux", "uy")]),
+              "itlbm_case_read_profile")
+        return out
+
 
 class Batch:
     """Many cases stepped together (itlbm_batch_* of include/itlbm.h)."""
@@ -362,6 +375,20 @@ class Batch:
         if n < 0:
             check(n, "itlbm_batch_poll")
         return [buf[i] for i in range(n)]
+
+    def hold_finished(self, on=True):
+        check(lib().itlbm_batch_hold_finished(self._h, 1 if on else 0), "itlbm_batch_hold_finished")
+
+    def read_fields(self, tag, n, form=FIELDS_VTK):
+        """Fields of an active case after a diagnostic step, or of a held finished case (n nodes)."""
+        out = {k: np.empty(n) for k in ("rho_R", "rho_B", "ux", "uy", "uz")}
+        check(lib().itlbm_batch_read_fields(self._h, tag, form, *[_dp(out[k]) for k in ("rho_R", "rho_B", "ux", "uy",
+                                                                                        "uz")]),
+              "itlbm_batch_read_fields")
+        return out
+
+    def release(self, tag):
+        check(lib().itlbm_batch_release(self._h, tag), "itlbm_batch_release")
 
     def stats(self) -> BatchStats:
         st = BatchStats()

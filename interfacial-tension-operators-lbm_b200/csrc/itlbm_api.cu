@@ -28,6 +28,10 @@ int cuda_fail(cudaError_t e, const char *what) {
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ITLBM_E_NODEVICE;
     return ITLBM_E_CUDA;
 }
+int use_device(int device) {
+    const cudaError_t e = cudaSetDevice(device);
+    return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "cudaSetDevice");
+}
 
 // Per-case parameters derived once on the host, with the reference's expressions so that the
 // device sees the same doubles the reference computes inline.
@@ -118,7 +122,6 @@ struct itlbm_case {
     double *aux = nullptr;
     double *tmp = nullptr;  // export / import staging (2 * 19 * n doubles)
     DiagScratch diag;
-    void *diag_out = nullptr;
     long long steps = 0;
     int aux_valid = 0;
     int device = 0;
@@ -197,14 +200,13 @@ int itlbm_operador_read(const char *path, itlbm_operador *op) {
 
 void itlbm_case_destroy(itlbm_case *c) {
     if (!c) return;
-    cudaSetDevice(c->device);
+    if (use_device(c->device) != ITLBM_OK) return;  // the device is gone: nothing left to free on it
     cudaDeviceSynchronize();
     if (c->dev) cudaFree(c->dev);
     if (c->tiles) cudaFree(c->tiles);
     if (c->mem) cudaFree(c->mem);
     if (c->aux) cudaFree(c->aux);
     if (c->tmp) cudaFree(c->tmp);
-    if (c->diag_out) cudaFree(c->diag_out);
     diag_free(c->diag);
     delete c;
 }
@@ -288,7 +290,7 @@ static int ensure_aux(itlbm_case *c) {
 int itlbm_case_step(itlbm_case *c, int nsteps, int flags, void *stream) {
     if (!c || nsteps < 0) return fail(ITLBM_E_ARG, "bad argument");
     if (nsteps == 0) return ITLBM_OK;
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     const bool keep = (flags & ITLBM_STEP_KEEP_AUX) != 0;
     if (keep) {
         int r = ensure_aux(c);
@@ -310,7 +312,7 @@ int itlbm_case_step(itlbm_case *c, int nsteps, int flags, void *stream) {
 
 int itlbm_case_sync(itlbm_case *c) {
     if (!c) return fail(ITLBM_E_ARG, "NULL case");
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "synchronize");
     if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
@@ -321,7 +323,7 @@ long long itlbm_case_steps_done(const itlbm_case *c) { return c ? c->steps : -1;
 
 int itlbm_case_save(itlbm_case *c, const char *path) {
     if (!c || !path) return fail(ITLBM_E_ARG, "NULL argument");
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     cudaError_t e = cudaDeviceSynchronize();  // steps may have gone to another stream
     if (e != cudaSuccess) return cuda_fail(e, "synchronize");
     return snap_write(path, c->desc, c->steps, c->host, c->host.buf[c->steps & 1]);
@@ -355,13 +357,8 @@ int itlbm_case_load(const char *path, itlbm_case **out) {
 }
 
 static int ensure_diag(itlbm_case *c) {
-    cudaError_t e = diag_alloc(c->diag, c->host.nx, c->host.ny);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(diagnostics)");
-    if (!c->diag_out) {
-        e = cudaMalloc(&c->diag_out, sizeof(itlbm_drop_diag) + sizeof(itlbm_strip_diag));
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(diag out)");
-    }
-    return ITLBM_OK;
+    const cudaError_t e = diag_alloc(c->diag, c->host.nx, c->host.ny);
+    return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "cudaMalloc(diagnostics)");
 }
 
 int itlbm_case_diag_drop(itlbm_case *c, int step, double x_ini, double y_ini, itlbm_drop_diag *out,
@@ -371,12 +368,12 @@ int itlbm_case_diag_drop(itlbm_case *c, int step, double x_ini, double y_ini, it
     const bool force = c->host.tipo >= ITLBM_OP_F1;
     if (force && !c->aux_valid)
         return fail(ITLBM_E_STATE, "class F: the last step must keep aux (ITLBM_STEP_KEEP_AUX)");
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     int r = ensure_diag(c);
     if (r) return r;
     cudaStream_t s = (cudaStream_t)stream;
     const int cur = (int)(c->steps & 1);
-    itlbm_drop_diag *od = (itlbm_drop_diag *)c->diag_out;
+    itlbm_drop_diag *od = (itlbm_drop_diag *)diag_scratch_out(c->diag);
     cudaError_t e = launch_diag_drop(c->dev, c->host, c->diag, cur, step, c->desc.v0, x_ini, y_ini,
                                      force, od, s);
     if (e != cudaSuccess) return cuda_fail(e, "diagnostic kernels");
@@ -403,8 +400,8 @@ int itlbm_case_diag_drop_static(itlbm_case *c, int step, double x_ini, double y_
     const bool force = c->host.tipo >= ITLBM_OP_F1;
     if (force && !c->aux_valid)
         return fail(ITLBM_E_STATE, "class F: the last step must keep aux (ITLBM_STEP_KEEP_AUX)");
-    cudaError_t e = cudaSetDevice(c->device);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    if (int rd = use_device(c->device)) return rd;
+    cudaError_t e;
     void *base = nullptr;
     size_t bytes = 0;
     if ((e = static_diag_scratch(c->device, &base, &bytes)) != cudaSuccess)
@@ -413,7 +410,7 @@ int itlbm_case_diag_drop_static(itlbm_case *c, int step, double x_ini, double y_
     if ((e = diag_bind(s, base, bytes, nx, ny)) != cudaSuccess)
         return fail(ITLBM_E_ARG, "itlbm_case_diag_drop_static: case does not fit the static scratch");
     cudaStream_t st = (cudaStream_t)stream;
-    itlbm_drop_diag *od = (itlbm_drop_diag *)s.out;
+    itlbm_drop_diag *od = (itlbm_drop_diag *)diag_scratch_out(s);
     e = launch_diag_drop(c->dev, c->host, s, (int)(c->steps & 1), step, c->desc.v0, x_ini, y_ini, force,
                          od, st);
     if (e != cudaSuccess) return cuda_fail(e, "diagnostic kernels");
@@ -429,12 +426,12 @@ int itlbm_case_diag_strip(itlbm_case *c, int step, itlbm_strip_diag *out, void *
     if (c->desc.geometry != ITLBM_GEOM_STRIP) return fail(ITLBM_E_STATE, "not a strip case");
     if (c->steps < 1) return fail(ITLBM_E_STATE, "no step has run yet");
     if (!c->aux_valid) return fail(ITLBM_E_STATE, "the last step must keep aux (ITLBM_STEP_KEEP_AUX)");
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     int r = ensure_diag(c);
     if (r) return r;
     cudaStream_t s = (cudaStream_t)stream;
     const int cur = (int)(c->steps & 1);
-    itlbm_strip_diag *od = (itlbm_strip_diag *)((char *)c->diag_out + sizeof(itlbm_drop_diag));
+    itlbm_strip_diag *od = (itlbm_strip_diag *)diag_scratch_out(c->diag);
     cudaError_t e = launch_diag_strip(c->dev, c->host, c->diag, cur, step, c->desc.p, c->desc.q,
                                       c->host.tipo >= ITLBM_OP_F1, od, s);
     if (e != cudaSuccess) return cuda_fail(e, "diagnostic kernels");
@@ -459,7 +456,7 @@ static int ensure_tmp(itlbm_case *c) {
 int itlbm_case_read_pops(itlbm_case *c, int which, double *fR, double *fB) {
     if (!c || !fR || !fB || (which != 0 && which != 1)) return fail(ITLBM_E_ARG, "bad argument");
     if (which == 1 && c->steps < 1) return fail(ITLBM_E_STATE, "no step has run yet");
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     int r = ensure_tmp(c);
     if (r) return r;
     const size_t n = (size_t)c->host.nx * c->host.ny;
@@ -473,7 +470,7 @@ int itlbm_case_read_pops(itlbm_case *c, int which, double *fR, double *fB) {
 
 int itlbm_case_write_pops(itlbm_case *c, const double *fR, const double *fB) {
     if (!c || !fR || !fB) return fail(ITLBM_E_ARG, "bad argument");
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     int r = ensure_tmp(c);
     if (r) return r;
     const size_t n = (size_t)c->host.nx * c->host.ny;
@@ -487,21 +484,22 @@ int itlbm_case_write_pops(itlbm_case *c, const double *fR, const double *fB) {
     return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "write_pops");
 }
 
-int itlbm_case_read_fields(itlbm_case *c, double *rho_R, double *rho_B, double *ux, double *uy,
-                           double *uz, double *force) {
+static int read_fields_as(itlbm_case *c, int form, double *rho_R, double *rho_B, double *ux, double *uy,
+                          double *uz, double *force) {
     if (!c) return fail(ITLBM_E_ARG, "NULL case");
     if (c->steps < 1) return fail(ITLBM_E_STATE, "no step has run yet");
     const bool cls_f = c->host.tipo >= ITLBM_OP_F1;
     if ((cls_f || force) && !c->aux_valid)
         return fail(ITLBM_E_STATE, "the last step must keep aux (ITLBM_STEP_KEEP_AUX)");
-    cudaSetDevice(c->device);
+    if (int rd = use_device(c->device)) return rd;
     int r = ensure_tmp(c);
     if (r) return r;
     const size_t n = (size_t)c->host.nx * c->host.ny;
     double *t = c->tmp;
     cudaError_t e = cudaDeviceSynchronize();  // steps may have gone to another stream
     if (e == cudaSuccess)
-        e = launch_fields(c->dev, c->host, (int)(c->steps & 1), cls_f, t, t + n, t + 2 * n, t + 3 * n, t + 4 * n, 0);
+        e = launch_fields(c->dev, c->host, (int)(c->steps & 1), cls_f, form, t, t + n, t + 2 * n, t + 3 * n,
+                          t + 4 * n, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     double *outs[5] = {rho_R, rho_B, ux, uy, uz};
     for (int k = 0; k < 5 && e == cudaSuccess; k++)
@@ -516,6 +514,15 @@ int itlbm_case_read_fields(itlbm_case *c, double *rho_R, double *rho_B, double *
             for (int k = 0; k < 3; k++) force[3 * p + k] = a[k * n + p];
     }
     return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "read_fields");
+}
+
+int itlbm_case_read_fields(itlbm_case *c, double *rho_R, double *rho_B, double *ux, double *uy,
+                           double *uz, double *force) {
+    return read_fields_as(c, ITLBM_FIELDS_VTK, rho_R, rho_B, ux, uy, uz, force);
+}
+
+int itlbm_case_read_profile(itlbm_case *c, double *rho_R, double *rho_B, double *ux, double *uy) {
+    return read_fields_as(c, ITLBM_FIELDS_PROFILE, rho_R, rho_B, ux, uy, nullptr, nullptr);
 }
 
 }  // extern "C"

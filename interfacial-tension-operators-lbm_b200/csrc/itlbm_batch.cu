@@ -59,6 +59,8 @@ struct Active {
     int parity = 0;     // buffer holding the state at next_step
     int chunk_len = 0;
     bool diag_at_end = false;
+    bool measured = false;  // its last advance ended at one of its diagnostic steps (aux kept there)
+    bool held = false;      // retired, state kept for itlbm_batch_read_fields until released
 };
 
 size_t case_bytes(const itlbm_case_desc &d, bool &need_aux) {
@@ -120,15 +122,22 @@ struct itlbm_batch {
     // join on `stream`: the tables hold different cases, so their steps need no order between them
     cudaStream_t side[NTAB] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[NTAB] = {};
-    DiagScratch diag;
-    int diag_nx = 0, diag_ny = 0;
-    itlbm_drop_diag *d_drop = nullptr;
-    itlbm_strip_diag *d_strip = nullptr;
-    std::vector<itlbm_drop_diag> h_drop;
-    std::vector<itlbm_strip_diag> h_strip;
+    // diagnostics: the cases that fall due in an advance are measured together, drops and strips each
+    // by one sequence of launches over a table of jobs, their scratch in per-case segments of one
+    // block (grown on demand, up to DIAG_SCRATCH_LIMIT or the largest single case; more due cases than
+    // that are measured in groups)
+    void *dscratch = nullptr;
+    size_t dscratch_cap = 0;
+    DiagJob *d_jobs = nullptr, *h_jobs = nullptr;  // one per slot at most in an advance (pinned host)
+    int *d_blk = nullptr, *h_blk = nullptr;        // block -> job maps of the full-field passes
+    size_t blk_cap = 0;
+    itlbm_drop_diag *d_drop = nullptr, *h_drop = nullptr;  // per slot (pinned host)
+    itlbm_strip_diag *d_strip = nullptr, *h_strip = nullptr;
     std::deque<itlbm_batch_event> events;
     std::chrono::steady_clock::time_point t0;
     size_t hbm_used = 0;
+    bool hold = false;  // retired cases are held until itlbm_batch_release
+    int nheld = 0;
     long long node_updates = 0;
     double device_ms = 0, diag_ms = 0, advance_ms = 0, admit_ms = 0, capture_ms = 0;
     int replays = 0, finished = 0, captures = 0;
@@ -164,7 +173,7 @@ void set_grids(itlbm_batch *b) {
 int upload_tables(itlbm_batch *b) {
     std::vector<TileRef> t[NTAB];
     for (Active *a : b->slots) {
-        if (!a) continue;
+        if (!a || a->held) continue;
         const CaseDev &c = b->h_cases[a->slot];
         const int p = table_of(a->desc.precision);
         const int n = case_items(c);
@@ -255,7 +264,7 @@ int capture_graph(itlbm_batch *b) {
 long long updates_in(const itlbm_batch *b, int k0, int k1) {
     long long u = 0;
     for (const Active *a : b->slots)
-        if (a) u += (long long)std::max(0, std::min(a->chunk_len, k1) - k0) * a->desc.nx * a->desc.ny;
+        if (a && !a->held) u += (long long)std::max(0, std::min(a->chunk_len, k1) - k0) * a->desc.nx * a->desc.ny;
     return u;
 }
 
@@ -288,15 +297,23 @@ int tune_and_run(itlbm_batch *b, int K) {
     return capture_graph(b);
 }
 
+// A retired case leaves the work table; with hold on it keeps its state until itlbm_batch_release.
 void retire(itlbm_batch *b, Active *a) {
+    b->tables_dirty = true;
+    b->finished++;
+    if (b->hold) {
+        a->held = true;
+        a->chunk_len = 0;
+        b->h_cases[a->slot].chunk_len = 0;
+        b->nheld++;
+        return;
+    }
     cudaFreeAsync(a->mem, b->stream);
     if (a->aux) cudaFreeAsync(a->aux, b->stream);
     b->hbm_used -= a->bytes;
     b->slots[a->slot] = nullptr;
     b->free_slots.push_back(a->slot);
     b->h_cases[a->slot] = CaseDev{};
-    b->tables_dirty = true;
-    b->finished++;
     delete a;
 }
 
@@ -433,6 +450,119 @@ int admit(itlbm_batch *b) {
     return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "initial states");
 }
 
+// Scratch of the diagnostics measured together: room for every due case, up to this many bytes (or
+// the largest single case); beyond it the due cases are measured in groups.
+constexpr size_t DIAG_SCRATCH_LIMIT = (size_t)4 << 30;
+
+// The diagnostics of the cases in `due` (their last sub-step of this replay is a diagnostic step),
+// enqueued on the batch stream: for each group of cases whose scratch fits, one table of drop jobs
+// and one of strip jobs, each measured by one sequence of launches.  Each job has its own scratch
+// segment and keeps the reduction order of the case alone.
+int run_diagnostics(itlbm_batch *b, const std::vector<Active *> &due) {
+    if (due.empty()) return ITLBM_OK;
+    size_t total = 0, largest = 0;
+    long long blocks = 0;
+    for (const Active *a : due) {
+        const size_t need = diag_job_bytes(a->desc.nx, a->desc.ny, a->desc.geometry);
+        total += need;
+        largest = std::max(largest, need);
+        blocks += diag_nblocks((long long)a->desc.nx * a->desc.ny);
+    }
+    cudaError_t e = cudaSuccess;
+    const size_t want = std::max(largest, std::min(total, DIAG_SCRATCH_LIMIT));
+    if (b->dscratch_cap < want) {
+        // grow (a device-wide synchronisation, rare: the first rounds of diagnostics); when the device
+        // has no room for all due cases, fall back to the largest single one
+        if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "synchronize");
+        void *p = nullptr;
+        for (size_t sz : {want, largest}) {
+            if (sz <= b->dscratch_cap) break;
+            if (cudaMalloc(&p, sz) == cudaSuccess) {
+                if (b->dscratch) cudaFree(b->dscratch);
+                b->dscratch = p;
+                b->dscratch_cap = sz;
+                break;
+            }
+            cudaGetLastError();
+        }
+        if (b->dscratch_cap < largest) return fail(ITLBM_E_OOM, "diagnostic scratch");
+    }
+    if ((size_t)blocks > b->blk_cap) {
+        if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "synchronize");
+        const size_t cap = std::max<size_t>((size_t)blocks, 2 * b->blk_cap);
+        if (b->d_blk) cudaFree(b->d_blk);
+        if (b->h_blk) cudaFreeHost(b->h_blk);
+        b->d_blk = nullptr;
+        b->h_blk = nullptr;
+        b->blk_cap = 0;
+        if ((e = cudaMalloc(&b->d_blk, sizeof(int) * cap)) != cudaSuccess ||
+            (e = cudaHostAlloc((void **)&b->h_blk, sizeof(int) * cap, cudaHostAllocDefault)) != cudaSuccess)
+            return cuda_fail(e, "diagnostic block map");
+        b->blk_cap = cap;
+    }
+    // the host tables of this advance are written once and copied in order; a group's copies are
+    // queued before its launches, and no later group reuses its part of the tables
+    int job_at = 0;
+    size_t blk_at = 0;
+    size_t k = 0;
+    while (k < due.size()) {
+        size_t used = 0, k1 = k;
+        while (k1 < due.size()) {
+            const Active *a = due[k1];
+            const size_t need = diag_job_bytes(a->desc.nx, a->desc.ny, a->desc.geometry);
+            if (used + need > b->dscratch_cap) break;
+            used += need;
+            k1++;
+        }
+        // this group: jobs [k, k1), scratch segments in order, drops then strips
+        size_t off = 0;
+        for (int geom : {ITLBM_GEOM_DROP, ITLBM_GEOM_STRIP}) {
+            const int j0 = job_at;
+            const size_t b0 = blk_at;
+            int nblk = 0;
+            size_t seg = 0;
+            for (size_t i = k; i < k1; i++) {
+                const Active *a = due[i];
+                const size_t need = diag_job_bytes(a->desc.nx, a->desc.ny, a->desc.geometry);
+                if (a->desc.geometry != geom) {
+                    seg += need;
+                    continue;
+                }
+                DiagJob &J = b->h_jobs[job_at];
+                J = DiagJob{};
+                diag_job_layout(J, (char *)b->dscratch + off + seg, a->desc.nx, a->desc.ny, geom);
+                seg += need;
+                J.c = b->d_cases + a->slot;
+                J.out = geom == ITLBM_GEOM_DROP ? (void *)(b->d_drop + a->slot) : (void *)(b->d_strip + a->slot);
+                J.cur = a->parity ^ (a->chunk_len & 1);
+                J.step = a->next_step + a->chunk_len - 1;
+                J.v0 = a->desc.v0;
+                J.x_ini = a->desc.nx / 2;
+                J.y_ini = a->desc.ny / 2;
+                J.use_force = a->desc.op.tipo >= ITLBM_OP_F1 ? 1 : 0;
+                J.p = a->desc.p;
+                J.q = a->desc.q;
+                J.block0 = nblk;
+                for (int q = 0; q < J.nblocks; q++) b->h_blk[blk_at + nblk + q] = job_at - j0;
+                nblk += J.nblocks;
+                job_at++;
+            }
+            const int nj = job_at - j0;
+            if (nj == 0) continue;
+            blk_at += nblk;
+            if ((e = cudaMemcpyAsync(b->d_jobs + j0, b->h_jobs + j0, sizeof(DiagJob) * nj, cudaMemcpyHostToDevice,
+                                     b->stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(b->d_blk + b0, b->h_blk + b0, sizeof(int) * nblk, cudaMemcpyHostToDevice,
+                                     b->stream)) != cudaSuccess ||
+                (e = launch_diag_jobs(b->d_jobs + j0, nj, b->d_blk + b0, nblk, geom, b->stream)) != cudaSuccess)
+                return cuda_fail(e, "diagnostics");
+        }
+        // the next group reuses the scratch: stream order keeps its launches after this group's
+        k = k1;
+    }
+    return ITLBM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -484,13 +614,15 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
     b->slots.assign(M, nullptr);
     for (int s = M - 1; s >= 0; s--) b->free_slots.push_back(s);
     b->h_cases.assign(M, CaseDev{});
-    b->h_drop.resize(M);
-    b->h_strip.resize(M);
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_cases, sizeof(CaseDev) * M)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_ntiles, sizeof(int) * NTAB)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_drop, sizeof(itlbm_drop_diag) * M)) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_strip, sizeof(itlbm_strip_diag) * M)) != cudaSuccess) {
+        (e = cudaMalloc(&b->d_strip, sizeof(itlbm_strip_diag) * M)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_jobs, sizeof(DiagJob) * M)) != cudaSuccess ||
+        (e = cudaHostAlloc((void **)&b->h_jobs, sizeof(DiagJob) * M, cudaHostAllocDefault)) != cudaSuccess ||
+        (e = cudaHostAlloc((void **)&b->h_drop, sizeof(itlbm_drop_diag) * M, cudaHostAllocDefault)) != cudaSuccess ||
+        (e = cudaHostAlloc((void **)&b->h_strip, sizeof(itlbm_strip_diag) * M, cudaHostAllocDefault)) != cudaSuccess) {
         itlbm_batch_destroy(b);
         return cuda_fail(e, "batch allocation");
     }
@@ -531,7 +663,7 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
 
 void itlbm_batch_destroy(itlbm_batch *b) {
     if (!b) return;
-    cudaSetDevice(b->device);
+    if (use_device(b->device) != ITLBM_OK) return;  // the device is gone: nothing left to free on it
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (Active *a : b->slots)
         if (a) {
@@ -547,7 +679,13 @@ void itlbm_batch_destroy(itlbm_batch *b) {
     if (b->d_ntiles) cudaFree(b->d_ntiles);
     if (b->d_drop) cudaFree(b->d_drop);
     if (b->d_strip) cudaFree(b->d_strip);
-    diag_free(b->diag);
+    if (b->d_jobs) cudaFree(b->d_jobs);
+    if (b->d_blk) cudaFree(b->d_blk);
+    if (b->dscratch) cudaFree(b->dscratch);
+    if (b->h_jobs) cudaFreeHost(b->h_jobs);
+    if (b->h_blk) cudaFreeHost(b->h_blk);
+    if (b->h_drop) cudaFreeHost(b->h_drop);
+    if (b->h_strip) cudaFreeHost(b->h_strip);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->ev2) cudaEventDestroy(b->ev2);
@@ -578,9 +716,9 @@ int itlbm_batch_submit_saved(itlbm_batch *b, const char *path, int n_steps, long
 
 int itlbm_batch_save(itlbm_batch *b, long long tag, const char *path) {
     if (!b || !path) return fail(ITLBM_E_ARG, "bad argument");
-    cudaSetDevice(b->device);
+    if (int rd = use_device(b->device)) return rd;
     for (Active *a : b->slots) {
-        if (!a || a->tag != tag) continue;
+        if (!a || a->held || a->tag != tag) continue;
         cudaError_t e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) return cuda_fail(e, "synchronize");
         const CaseDev &h = b->h_cases[a->slot];
@@ -607,7 +745,7 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
     (void)stream;  // the batch runs on its own stream (graphs cannot be captured on the legacy one)
     if (!b) return fail(ITLBM_E_ARG, "NULL batch");
     ScopeTimer timer(b, b->advance_ms);
-    cudaSetDevice(b->device);
+    if (int rd = use_device(b->device)) return rd;
     int r;
     {
         ScopeTimer t_admit(b, b->admit_ms);
@@ -619,7 +757,7 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
     int K = 0, hi = -1;
     long long updates = 0;
     for (Active *a : b->slots) {
-        if (!a) continue;
+        if (!a || a->held) continue;
         hi = std::max(hi, a->slot);
         int d = ((a->next_step + de - 1) / de) * de;  // next multiple of diag_every >= next_step
         if (d > a->n_steps - 1) d = a->n_steps - 1;
@@ -667,57 +805,31 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
     cudaEventRecord(b->ev1, b->stream);
     b->replays++;
     b->node_updates += updates;
-    // diagnostics that fell due
+    // diagnostics that fell due, all of them together
     std::vector<Active *> measured;
-    for (Active *a : b->slots) {
-        if (!a || !a->diag_at_end) continue;
-        if (a->desc.nx > b->diag_nx || a->desc.ny > b->diag_ny) {
-            // one scratch for every case, sized by the largest box seen (diagnostics run in turn)
-            cudaStreamSynchronize(b->stream);
-            b->diag_nx = std::max(b->diag_nx, a->desc.nx);
-            b->diag_ny = std::max(b->diag_ny, a->desc.ny);
-            e = diag_alloc(b->diag, b->diag_nx, b->diag_ny);
-            if (e != cudaSuccess) return cuda_fail(e, "diagnostic scratch");
-        }
-        // the scratch is sized for the largest case; the kernels only use the first n entries, but
-        // the shell histogram length depends on the box diagonal, so re-derive it per case
-        DiagScratch s = b->diag;
-        s.n = a->desc.nx * a->desc.ny;
-        s.nshell = (int)(sqrt((double)(a->desc.nx * a->desc.nx + a->desc.ny * a->desc.ny + 1)) / 0.5) + 2;
-        {
-            long long nb = ((long long)s.n + 255) / 256;
-            s.nblocks = (int)std::max(1LL, std::min(nb, (long long)148 * 8));
-        }
-        const int step = a->next_step + a->chunk_len - 1;
-        const int cur = a->parity ^ (a->chunk_len & 1);
-        const CaseDev &h = b->h_cases[a->slot];
-        if (a->desc.geometry == ITLBM_GEOM_DROP)
-            e = launch_diag_drop(b->d_cases + a->slot, h, s, cur, step, a->desc.v0, a->desc.nx / 2,
-                                 a->desc.ny / 2, a->desc.op.tipo >= ITLBM_OP_F1, b->d_drop + a->slot, b->stream);
-        else
-            e = launch_diag_strip(b->d_cases + a->slot, h, s, cur, step, a->desc.p, a->desc.q,
-                                  a->desc.op.tipo >= ITLBM_OP_F1, b->d_strip + a->slot, b->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "diagnostics");
-        measured.push_back(a);
-    }
+    for (Active *a : b->slots)
+        if (a && !a->held && a->diag_at_end) measured.push_back(a);
+    if ((r = run_diagnostics(b, measured)) != ITLBM_OK) return r;
     cudaEventRecord(b->ev2, b->stream);
-    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "replay");
-    if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
-    float ms = 0;
-    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-    b->device_ms += ms;
-    if (!measured.empty() && cudaEventElapsedTime(&ms, b->ev1, b->ev2) == cudaSuccess) b->diag_ms += ms;
     if (!measured.empty()) {
         int lo = INT_MAX, hi = -1;
         for (Active *a : measured) {
             lo = std::min(lo, a->slot);
             hi = std::max(hi, a->slot);
         }
-        e = cudaMemcpy(b->h_drop.data() + lo, b->d_drop + lo, sizeof(itlbm_drop_diag) * (hi - lo + 1), cudaMemcpyDeviceToHost);
+        e = cudaMemcpyAsync(b->h_drop + lo, b->d_drop + lo, sizeof(itlbm_drop_diag) * (hi - lo + 1),
+                            cudaMemcpyDeviceToHost, b->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpy(b->h_strip.data() + lo, b->d_strip + lo, sizeof(itlbm_strip_diag) * (hi - lo + 1), cudaMemcpyDeviceToHost);
+            e = cudaMemcpyAsync(b->h_strip + lo, b->d_strip + lo, sizeof(itlbm_strip_diag) * (hi - lo + 1),
+                                cudaMemcpyDeviceToHost, b->stream);
         if (e != cudaSuccess) return cuda_fail(e, "diagnostic copy");
     }
+    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "replay");
+    if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->device_ms += ms;
+    if (!measured.empty() && cudaEventElapsedTime(&ms, b->ev1, b->ev2) == cudaSuccess) b->diag_ms += ms;
     const double t = b->now();
     std::vector<Active *> gone;
     for (Active *a : measured) {
@@ -748,12 +860,66 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         }
     }
     for (Active *a : b->slots) {
-        if (!a) continue;
+        if (!a || a->held) continue;
         a->next_step += a->chunk_len;
         a->parity ^= (a->chunk_len & 1);
+        a->measured = a->diag_at_end;
     }
     for (Active *a : gone) retire(b, a);
     return (int)b->events.size();
+}
+
+int itlbm_batch_hold_finished(itlbm_batch *b, int on) {
+    if (!b) return fail(ITLBM_E_ARG, "NULL batch");
+    b->hold = on != 0;
+    return ITLBM_OK;
+}
+
+namespace {
+Active *find_tag(itlbm_batch *b, long long tag) {
+    for (Active *a : b->slots)
+        if (a && a->tag == tag) return a;
+    return nullptr;
+}
+}  // namespace
+
+int itlbm_batch_read_fields(itlbm_batch *b, long long tag, int form, double *rho_R, double *rho_B,
+                            double *ux, double *uy, double *uz) {
+    if (!b || (form != ITLBM_FIELDS_VTK && form != ITLBM_FIELDS_PROFILE)) return fail(ITLBM_E_ARG, "bad argument");
+    Active *a = find_tag(b, tag);
+    if (!a) return fail(ITLBM_E_ARG, "no active or held case with this tag");
+    const bool force = a->desc.op.tipo >= ITLBM_OP_F1;
+    if (a->next_step < 1 || (force && !a->measured))
+        return fail(ITLBM_E_STATE, "the case's last step was not a measured one (class F needs its force)");
+    if (int rd = use_device(b->device)) return rd;
+    const size_t n = (size_t)a->desc.nx * a->desc.ny;
+    double *t = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&t, sizeof(double) * 5 * n, b->pool, b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "field staging");
+    // the post-collision populations of the last step sit in the buffer of the next step's state
+    e = launch_fields(b->d_cases + a->slot, b->h_cases[a->slot], a->parity, force, form, t, t + n, t + 2 * n,
+                      t + 3 * n, t + 4 * n, b->stream);
+    double *outs[5] = {rho_R, rho_B, ux, uy, uz};
+    for (int k = 0; k < 5 && e == cudaSuccess; k++)
+        if (outs[k]) e = cudaMemcpyAsync(outs[k], t + k * n, sizeof(double) * n, cudaMemcpyDeviceToHost, b->stream);
+    cudaFreeAsync(t, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "read_fields");
+}
+
+int itlbm_batch_release(itlbm_batch *b, long long tag) {
+    if (!b) return fail(ITLBM_E_ARG, "NULL batch");
+    Active *a = find_tag(b, tag);
+    if (!a || !a->held) return fail(ITLBM_E_ARG, "no held case with this tag");
+    if (int rd = use_device(b->device)) return rd;
+    a->held = false;
+    b->nheld--;
+    const bool hold = b->hold;
+    b->hold = false;
+    b->finished--;  // retire() counts it again
+    retire(b, a);
+    b->hold = hold;
+    return ITLBM_OK;
 }
 
 int itlbm_batch_poll(itlbm_batch *b, itlbm_batch_event *ev, int max) {
@@ -769,7 +935,8 @@ int itlbm_batch_poll(itlbm_batch *b, itlbm_batch_event *ev, int max) {
 int itlbm_batch_stats_get(const itlbm_batch *b, itlbm_batch_stats *out) {
     if (!b || !out) return fail(ITLBM_E_ARG, "bad argument");
     out->active = 0;
-    for (Active *a : b->slots) out->active += a ? 1 : 0;
+    for (Active *a : b->slots) out->active += (a && !a->held) ? 1 : 0;
+    out->held = b->nheld;
     out->pending = (int)b->pending.size();
     out->finished = b->finished;
     out->node_updates = b->node_updates;

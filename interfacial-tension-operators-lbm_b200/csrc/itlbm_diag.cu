@@ -22,6 +22,7 @@
 #include "itlbm_site.cuh"
 
 #include <cfloat>
+#include <math_constants.h>
 
 namespace itlbm {
 
@@ -118,9 +119,22 @@ __device__ __forceinline__ void init_acc(double (&v)[Q]) {
     for (int q = 0; q < Q; q++) v[q] = (q < NS) ? 0.0 : (q < NS + NM ? -DBL_MAX : DBL_MAX);
 }
 
-// Reduce nb partials (rows of Q) in block order into res[0..Q).
+// The job of this block of a full-field pass and the block's index within the job: a table of jobs
+// with a block -> job map, or the single job passed by value (jobs == nullptr).
+__device__ __forceinline__ const DiagJob &block_job(const DiagJob *jobs, const int *blk_job,
+                                                    const DiagJob &one, int &lb) {
+    if (!jobs) {
+        lb = blockIdx.x;
+        return one;
+    }
+    const DiagJob &J = jobs[blk_job[blockIdx.x]];
+    lb = blockIdx.x - J.block0;
+    return J;
+}
+
+// Reduce nb partials (rows of Q) in block order into res[0..Q) (one block).
 template <int Q, int NS, int NM>
-__global__ void k_reduce(const double *__restrict__ part, int nb, double *__restrict__ res) {
+__device__ void reduce_rows(const double *__restrict__ part, int nb, double *__restrict__ res) {
     double v[Q];
     init_acc<Q, NS, NM>(v);
     for (int b = threadIdx.x; b < nb; b += DT) {
@@ -167,17 +181,21 @@ struct DropState {
     double fit[6];
 };
 
-__global__ void __launch_bounds__(DT) k_drop_d1(const CaseDev *__restrict__ cp, int cur,
-                                                int use_force, double *__restrict__ node,
-                                                double *__restrict__ part) {
-    const CaseDev &c = *cp;
+__global__ void __launch_bounds__(DT) k_drop_d1(const DiagJob *__restrict__ jobs,
+                                                const int *__restrict__ blk_job,
+                                                const __grid_constant__ DiagJob one) {
+    int lb;
+    const DiagJob &J = block_job(jobs, blk_job, one, lb);
+    const CaseDev &c = *J.c;
+    const int cur = J.cur, use_force = J.use_force, nb = J.nblocks;
+    double *__restrict__ node = J.node;
     const int nx = c.nx, ny = c.ny;
     const long long n = (long long)nx * ny;
     const double pi = 3.14159265358979323846;
     const double tx = 2.0 * pi / (double)nx, ty = 2.0 * pi / (double)ny;
     double v[A_Q];
     init_acc<A_Q, A_NS, A_NM>(v);
-    for (long long p = blockIdx.x * (long long)DT + threadIdx.x; p < n; p += (long long)gridDim.x * DT) {
+    for (long long p = lb * (long long)DT + threadIdx.x; p < n; p += (long long)nb * DT) {
         const int x = (int)(p % nx), y = (int)(p / nx);
         double fR[NV], fB[NV];
         post_pops(c, cur, x, y, fR, fB);
@@ -303,12 +321,16 @@ __global__ void __launch_bounds__(DT) k_drop_d1(const CaseDev *__restrict__ cp, 
         v[A_CYC] += phi * cos(ty * y);
         v[A_CYS] += phi * sin(ty * y);
     }
-    block_reduce<A_Q, A_NS, A_NM>(v, part + (long long)blockIdx.x * A_Q);
+    block_reduce<A_Q, A_NS, A_NM>(v, J.part + (long long)lb * A_Q);
 }
 
-__global__ void k_drop_f1(const CaseDev *__restrict__ cp, DropState *__restrict__ st,
-                          itlbm_drop_diag *__restrict__ d) {
-    const CaseDev &c = *cp;
+__global__ void k_drop_f1(const DiagJob *__restrict__ jobs, int njobs, const __grid_constant__ DiagJob one) {
+    const int jid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jid >= njobs) return;
+    const DiagJob &J = jobs ? jobs[jid] : one;
+    const CaseDev &c = *J.c;
+    DropState *__restrict__ st = (DropState *)J.state;
+    itlbm_drop_diag *__restrict__ d = (itlbm_drop_diag *)J.out;
     const double *a = st->a;
     const int nx = c.nx, ny = c.ny;
     const double pi = 3.14159265358979323846;
@@ -371,14 +393,19 @@ __device__ __forceinline__ double min_image(double dx, int L) {
 }
 __device__ __forceinline__ double gi_image(double dx, double L) { return dx - L * floor(dx / L + 0.5); }
 
-__global__ void __launch_bounds__(DT) k_drop_d2(const CaseDev *__restrict__ cp,
-                                                const DropState *__restrict__ st,
-                                                const itlbm_drop_diag *__restrict__ d, double v0,
-                                                const double *__restrict__ node,
-                                                double *__restrict__ part,
-                                                unsigned long long *__restrict__ shell, int nshell) {
+__global__ void __launch_bounds__(DT) k_drop_d2(const DiagJob *__restrict__ jobs,
+                                                const int *__restrict__ blk_job,
+                                                const __grid_constant__ DiagJob one) {
+    int lb;
+    const DiagJob &J = block_job(jobs, blk_job, one, lb);
+    const DropState *__restrict__ st = (const DropState *)J.state;
     if (!st->proceed) return;
-    const CaseDev &c = *cp;
+    const itlbm_drop_diag *__restrict__ d = (const itlbm_drop_diag *)J.out;
+    const double v0 = J.v0;
+    const double *__restrict__ node = J.node;
+    unsigned long long *__restrict__ shell = J.shell;
+    const int nshell = J.nshell, nb = J.nblocks;
+    const CaseDev &c = *J.c;
     const int nx = c.nx, ny = c.ny;
     const long long n = (long long)nx * ny;
     const double x0 = d->x0, y0 = d->y0;
@@ -387,7 +414,7 @@ __global__ void __launch_bounds__(DT) k_drop_d2(const CaseDev *__restrict__ cp,
     const double r_in_max = st->r_in_max, r_out_min = st->r_out_min;
     double v[B_Q];
     init_acc<B_Q, B_NS, B_NM>(v);
-    for (long long p = blockIdx.x * (long long)DT + threadIdx.x; p < n; p += (long long)gridDim.x * DT) {
+    for (long long p = lb * (long long)DT + threadIdx.x; p < n; p += (long long)nb * DT) {
         const int x = (int)(p % nx), y = (int)(p / nx);
         const double rho_R = node[p], rho_B = node[n + p];
         const double ux = node[2 * n + p], uy = node[3 * n + p], uz = node[4 * n + p];
@@ -442,14 +469,20 @@ __global__ void __launch_bounds__(DT) k_drop_d2(const CaseDev *__restrict__ cp,
             }
         }
     }
-    block_reduce<B_Q, B_NS, B_NM>(v, part + (long long)blockIdx.x * B_Q);
+    block_reduce<B_Q, B_NS, B_NM>(v, J.part + (long long)lb * B_Q);
 }
 
-__global__ void k_drop_f2(const CaseDev *__restrict__ cp, DropState *__restrict__ st,
-                          itlbm_drop_diag *__restrict__ d, int step, double v0, double x_ini,
-                          double y_ini, const double *__restrict__ node) {
+__global__ void k_drop_f2(const DiagJob *__restrict__ jobs, int njobs, const __grid_constant__ DiagJob one) {
+    const int jid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jid >= njobs) return;
+    const DiagJob &J = jobs ? jobs[jid] : one;
+    DropState *__restrict__ st = (DropState *)J.state;
     if (!st->proceed) return;
-    const CaseDev &c = *cp;
+    itlbm_drop_diag *__restrict__ d = (itlbm_drop_diag *)J.out;
+    const int step = J.step;
+    const double v0 = J.v0, x_ini = J.x_ini, y_ini = J.y_ini;
+    const double *__restrict__ node = J.node;
+    const CaseDev &c = *J.c;
     const int nx = c.nx, ny = c.ny;
     const long long n = (long long)nx * ny;
     const double *b = st->b;
@@ -503,11 +536,14 @@ __global__ void k_drop_f2(const CaseDev *__restrict__ cp, DropState *__restrict_
 }
 
 // calc_perfil_logistico's fit over the shells (one block)
-__global__ void __launch_bounds__(DT) k_drop_fit(DropState *__restrict__ st,
-                                                 itlbm_drop_diag *__restrict__ d,
-                                                 const unsigned long long *__restrict__ shell,
-                                                 int nshell) {
+__global__ void __launch_bounds__(DT) k_drop_fit(const DiagJob *__restrict__ jobs,
+                                                 const __grid_constant__ DiagJob one) {
+    const DiagJob &J = jobs ? jobs[blockIdx.x] : one;
+    DropState *__restrict__ st = (DropState *)J.state;
     if (!st->proceed) return;
+    itlbm_drop_diag *__restrict__ d = (itlbm_drop_diag *)J.out;
+    const unsigned long long *__restrict__ shell = J.shell;
+    const int nshell = J.nshell;
     const double eps = 1.0e-30, d_casca = 0.5;
     double v[6];
     init_acc<6, 6, 0>(v);
@@ -589,37 +625,78 @@ __device__ double fase_em(const double *__restrict__ node, long long n, int nx, 
     return v;
 }
 
-__global__ void __launch_bounds__(ITLBM_N_ANG) k_drop_modes(const CaseDev *__restrict__ cp,
-                                                            const DropState *__restrict__ st,
-                                                            itlbm_drop_diag *__restrict__ d,
-                                                            const double *__restrict__ node) {
+// modos_interface: one warp per ray.  The reference bisects 60 times from [0.3 R, 1.7 R], keeping the
+// sign of rho^N at the inner end; here each round evaluates, one point per lane, all 31 midpoints the
+// next five bisections can visit (the 5-level tree under the current interval, each midpoint formed
+// from its interval exactly as the serial bisection forms it), then walks the tree by the signs.  The
+// 12 rounds take the same path and give the same interval, bit for bit, with 12 dependent
+// evaluations instead of 60.
+constexpr int RAYS_PER_BLOCK = DT / 32;
+constexpr int MODE_BLOCKS = ITLBM_N_ANG / RAYS_PER_BLOCK;  // blocks per job
+__global__ void __launch_bounds__(DT) k_drop_modes(const DiagJob *__restrict__ jobs,
+                                                   const __grid_constant__ DiagJob one) {
+    const DiagJob &J = jobs ? jobs[blockIdx.x / MODE_BLOCKS] : one;
+    const DropState *__restrict__ st = (const DropState *)J.state;
     if (!st->proceed) return;
-    const CaseDev &c = *cp;
+    const itlbm_drop_diag *__restrict__ d = (const itlbm_drop_diag *)J.out;
+    const CaseDev &c = *J.c;
     const int nx = c.nx, ny = c.ny;
     const long long n = (long long)nx * ny;
+    const double *__restrict__ node = J.node;
     const int N_ANG = ITLBM_N_ANG;
+    const int lane = threadIdx.x & 31;
+    const int k = (blockIdx.x % MODE_BLOCKS) * RAYS_PER_BLOCK + (threadIdx.x >> 5);
     const double x0 = d->x0, y0 = d->y0, R_est = d->raio;
-    const int k = threadIdx.x;
     const double th = 2.0 * 3.14159265358979323846 * k / N_ANG, ct = cos(th), st_ = sin(th);
     double a = 0.3 * R_est, b = 1.7 * R_est;
-    const double fa = fase_em(node, n, nx, ny, x0 + a * ct, y0 + a * st_);
-    for (int it = 0; it < 60; it++) {
-        const double mid = 0.5 * (a + b);
-        const double fm = fase_em(node, n, nx, ny, x0 + mid * ct, y0 + mid * st_);
-        if ((fm > 0) == (fa > 0)) a = mid;
-        else b = mid;
+    const bool pos_a = fase_em(node, n, nx, ny, x0 + a * ct, y0 + a * st_) > 0;
+    const int h = lane + 1;             // tree node of this lane (heap order; lane 31 idle)
+    const int depth = 31 - __clz(h);
+    for (int round = 0; round < 12; round++) {
+        double lo = a, hi = b;
+        for (int l = depth - 1; l >= 0; l--) {
+            const double m = 0.5 * (lo + hi);
+            if ((h >> l) & 1) lo = m;
+            else hi = m;
+        }
+        const double mid = 0.5 * (lo + hi);
+        bool right = false;
+        if (lane < 31) right = (fase_em(node, n, nx, ny, x0 + mid * ct, y0 + mid * st_) > 0) == pos_a;
+        const unsigned go_right = __ballot_sync(0xffffffffu, right);
+        int v = 1;
+        for (int l = 0; l < 5; l++) {
+            const double m = __shfl_sync(0xffffffffu, mid, v - 1);
+            const int r = (go_right >> (v - 1)) & 1;
+            if (r) a = m;
+            else b = m;
+            v = 2 * v + r;
+        }
     }
-    const double r = 0.5 * (a + b);
-    // each ray forms its own harmonic products; one thread then sums them in ray order, as the
-    // reference loop does
+    if (lane == 0) {
+        const double r = 0.5 * (a + b);
+        double *__restrict__ rs = J.rays;
+        rs[0 * N_ANG + k] = r;
+        rs[1 * N_ANG + k] = r * cos(2 * th);
+        rs[2 * N_ANG + k] = r * sin(2 * th);
+        rs[3 * N_ANG + k] = r * cos(4 * th);
+        rs[4 * N_ANG + k] = r * sin(4 * th);
+        rs[5 * N_ANG + k] = r * cos(8 * th);
+        rs[6 * N_ANG + k] = r * sin(8 * th);
+    }
+}
+
+// The harmonic sums over the rays in ray order, as the reference loop accumulates them (one block
+// per job).
+__global__ void __launch_bounds__(ITLBM_N_ANG) k_drop_modes_sum(const DiagJob *__restrict__ jobs,
+                                                                const __grid_constant__ DiagJob one) {
+    const DiagJob &J = jobs ? jobs[blockIdx.x] : one;
+    if (!((const DropState *)J.state)->proceed) return;
+    itlbm_drop_diag *__restrict__ d = (itlbm_drop_diag *)J.out;
+    const int N_ANG = ITLBM_N_ANG;
     __shared__ double rs[7][ITLBM_N_ANG];
-    rs[0][k] = r;
-    rs[1][k] = r * cos(2 * th);
-    rs[2][k] = r * sin(2 * th);
-    rs[3][k] = r * cos(4 * th);
-    rs[4][k] = r * sin(4 * th);
-    rs[5][k] = r * cos(8 * th);
-    rs[6][k] = r * sin(8 * th);
+    const int k = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 7; q++) rs[q][k] = J.rays[q * N_ANG + k];
     __syncthreads();
     if (k == 0) {
         double c2 = 0, s2 = 0, c4 = 0, s4 = 0, c8 = 0, s8 = 0, soma = 0, rmin = 1e30, rmax = 0;
@@ -642,6 +719,16 @@ __global__ void __launch_bounds__(ITLBM_N_ANG) k_drop_modes(const CaseDev *__res
         d->rmin = rmin;
         d->rmax = rmax;
     }
+}
+
+// Clears what a drop diagnostic accumulates into: its output and its shell histogram (one block per
+// job).
+__global__ void __launch_bounds__(DT) k_drop_clear(const DiagJob *__restrict__ jobs,
+                                                   const __grid_constant__ DiagJob one) {
+    const DiagJob &J = jobs ? jobs[blockIdx.x] : one;
+    unsigned *o = (unsigned *)J.out;
+    for (int w = threadIdx.x; w < (int)(sizeof(itlbm_drop_diag) / 4); w += DT) o[w] = 0u;
+    for (int w = threadIdx.x; w < 2 * J.nshell; w += DT) J.shell[w] = 0ull;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -673,16 +760,20 @@ __device__ __forceinline__ double dist_central(int x, int y, int p, int q, int N
     return -d / m;
 }
 
-__global__ void __launch_bounds__(DT) k_strip_s1(const CaseDev *__restrict__ cp, int cur, int p,
-                                                 int q, int use_force, double *__restrict__ part) {
-    const CaseDev &c = *cp;
+__global__ void __launch_bounds__(DT) k_strip_s1(const DiagJob *__restrict__ jobs,
+                                                 const int *__restrict__ blk_job,
+                                                 const __grid_constant__ DiagJob one) {
+    int lb;
+    const DiagJob &J = block_job(jobs, blk_job, one, lb);
+    const CaseDev &c = *J.c;
+    const int cur = J.cur, p = J.p, q = J.q, use_force = J.use_force, nb = J.nblocks;
     const int N = c.nx;
     const long long n = (long long)N * N;
     const double m = sqrt((double)(p * p + q * q));
     const double nx_ = p / m, ny_ = q / m, tx_ = -ny_, ty_ = nx_;
     double v[S_Q];
     init_acc<S_Q, S_NS, S_NM>(v);
-    for (long long t = blockIdx.x * (long long)DT + threadIdx.x; t < n; t += (long long)gridDim.x * DT) {
+    for (long long t = lb * (long long)DT + threadIdx.x; t < n; t += (long long)nb * DT) {
         const int x = (int)(t % N), y = (int)(t / N);
         double fR[NV], fB[NV];
         post_pops(c, cur, x, y, fR, fB);
@@ -745,12 +836,17 @@ __global__ void __launch_bounds__(DT) k_strip_s1(const CaseDev *__restrict__ cp,
             v[S_NFIT] += 1.0;
         }
     }
-    block_reduce<S_Q, S_NS, S_NM>(v, part + (long long)blockIdx.x * S_Q);
+    block_reduce<S_Q, S_NS, S_NM>(v, J.part + (long long)lb * S_Q);
 }
 
-__global__ void k_strip_f1(const CaseDev *__restrict__ cp, StripState *__restrict__ st, int p, int q,
-                           itlbm_strip_diag *__restrict__ r) {
-    const int N = cp->nx;
+__global__ void k_strip_f1(const DiagJob *__restrict__ jobs, int njobs, const __grid_constant__ DiagJob one) {
+    const int jid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jid >= njobs) return;
+    const DiagJob &J = jobs ? jobs[jid] : one;
+    StripState *__restrict__ st = (StripState *)J.state;
+    itlbm_strip_diag *__restrict__ r = (itlbm_strip_diag *)J.out;
+    const int p = J.p, q = J.q;
+    const int N = J.c->nx;
     const double *a = st->a;
     const double m = sqrt((double)(p * p + q * q));
     const double comprimento = 2.0 * N * m;
@@ -789,17 +885,20 @@ __global__ void k_strip_f1(const CaseDev *__restrict__ cp, StripState *__restric
     r->ok = (r->n_ruim == 0 && isfinite(r->u_max));
 }
 
-__global__ void __launch_bounds__(DT) k_strip_s2(const CaseDev *__restrict__ cp, int cur, int p,
-                                                 int q, const StripState *__restrict__ st,
-                                                 double *__restrict__ part) {
+__global__ void __launch_bounds__(DT) k_strip_s2(const DiagJob *__restrict__ jobs,
+                                                 const int *__restrict__ blk_job,
+                                                 const __grid_constant__ DiagJob one) {
+    int lb;
+    const DiagJob &J = block_job(jobs, blk_job, one, lb);
+    const StripState *__restrict__ st = (const StripState *)J.state;
+    const int cur = J.cur, p = J.p, q = J.q, nb = J.nblocks;
     double m[1] = {0.0};
     if (st->fit) {
-        const CaseDev &c = *cp;
+        const CaseDev &c = *J.c;
         const int N = c.nx;
         const long long n = (long long)N * N;
         const double K = st->K, a0 = st->a0;
-        for (long long t = blockIdx.x * (long long)DT + threadIdx.x; t < n;
-             t += (long long)gridDim.x * DT) {
+        for (long long t = lb * (long long)DT + threadIdx.x; t < n; t += (long long)nb * DT) {
             const int x = (int)(t % N), y = (int)(t / N);
             double fR[NV], fB[NV];
             post_pops(c, cur, x, y, fR, fB);
@@ -818,16 +917,53 @@ __global__ void __launch_bounds__(DT) k_strip_s2(const CaseDev *__restrict__ cp,
             }
         }
     }
-    block_reduce<1, 0, 1>(m, part + blockIdx.x);
+    block_reduce<1, 0, 1>(m, J.part + lb);
 }
 
-__global__ void k_strip_f2(StripState *__restrict__ st, itlbm_strip_diag *__restrict__ r) {
+__global__ void k_strip_f2(const DiagJob *__restrict__ jobs, int njobs, const __grid_constant__ DiagJob one) {
+    const int jid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jid >= njobs) return;
+    const DiagJob &J = jobs ? jobs[jid] : one;
+    const StripState *__restrict__ st = (const StripState *)J.state;
+    itlbm_strip_diag *__restrict__ r = (itlbm_strip_diag *)J.out;
     if (st->fit) r->res = st->res[0] < 0 ? 0.0 : st->res[0];
 }
 
-// per-node fields of the post-collision state (rec_density / rec_velocity / perfil.dat)
-__global__ void k_fields(const CaseDev *__restrict__ cp, int cur, int use_force, double *rR_out,
-                         double *rB_out, double *ux_out, double *uy_out, double *uz_out) {
+__global__ void __launch_bounds__(DT) k_strip_clear(const DiagJob *__restrict__ jobs,
+                                                    const __grid_constant__ DiagJob one) {
+    const DiagJob &J = jobs ? jobs[blockIdx.x] : one;
+    unsigned *o = (unsigned *)J.out;
+    for (int w = threadIdx.x; w < (int)(sizeof(itlbm_strip_diag) / 4); w += DT) o[w] = 0u;
+}
+
+// The block reductions of the partials, one block per job, into the job's running state.
+enum { R_DROP_A, R_DROP_B, R_STRIP_A, R_STRIP_RES };
+template <int Q, int NS, int NM, int W>
+__global__ void __launch_bounds__(DT) k_reduce_jobs(const DiagJob *__restrict__ jobs,
+                                                    const __grid_constant__ DiagJob one) {
+    const DiagJob &J = jobs ? jobs[blockIdx.x] : one;
+    double *res;
+    if constexpr (W == R_DROP_A) res = ((DropState *)J.state)->a;
+    else if constexpr (W == R_DROP_B) res = ((DropState *)J.state)->b;
+    else if constexpr (W == R_STRIP_A) res = ((StripState *)J.state)->a;
+    else res = ((StripState *)J.state)->res;
+    reduce_rows<Q, NS, NM>(J.part, J.nblocks, res);
+}
+
+// Per-node output fields of the post-collision state, each value formed with the reference's
+// operations in its order and rounded as written (the __d*_rn intrinsics keep the compiler from
+// contracting a product and a sum into one FMA, which would round differently):
+//   rho_R, rho_B   density() of each colour, index order (LBM_functions.cpp:1582-1590);
+//   FIELDS_VTK     rec_velocity's two-colour branch (LBM_functions.cpp:1349-1458): u_C = m_C * (1 / rho_C)
+//                  by calcula (:1100-1171) for each colour, u = c_R u_R + c_B u_B with c_B = 1 - c_R,
+//                  then u -= (0.5 F) / rho for a case with a force (rho > 0);
+//   FIELDS_PROFILE perfil.dat of mede_inclinada (Imm_INCL.cpp:104-162): u = (sum_i f_i c_i - 0.5 F) / rho
+//                  with f_i = f_R,i + f_B,i; a node with !(rho > 0) is skipped there and gets NaN here.
+// Sums of +-f over the non-zero components of c_i equal the reference's sums of c_i * f (the zero
+// terms add a signed zero, which changes no finite partial sum).
+__global__ void k_fields(const CaseDev *__restrict__ cp, int cur, int use_force, int form,
+                         double *rR_out, double *rB_out, double *ux_out, double *uy_out,
+                         double *uz_out) {
     const CaseDev &c = *cp;
     const int nx = c.nx;
     const long long n = (long long)nx * c.ny;
@@ -836,27 +972,79 @@ __global__ void k_fields(const CaseDev *__restrict__ cp, int cur, int use_force,
         const int x = (int)(p % nx), y = (int)(p / nx);
         double fR[NV], fB[NV];
         post_pops(c, cur, x, y, fR, fB);
-        double rr = 0, rb = 0, mx = 0, my = 0, mz = 0;
-        for (int i = 0; i < NV; i++) {
-            const double f = fR[i] + fB[i];
-            rr += fR[i];
-            rb += fB[i];
-            mx += f * cx(i);
-            my += f * cy(i);
-            mz += f * cz(i);
-        }
-        const double rho = rr + rb;
-        if (use_force && rho > 0.0) {
-            const long long o = (long long)y * c.pitch + x;
-            mx -= 0.5 * c.aux[o];
-            my -= 0.5 * c.aux[c.stride + o];
-            mz -= 0.5 * c.aux[2 * c.stride + o];
+        double rr = 0.0, rb = 0.0;
+#pragma unroll
+        for (int i = 0; i < NV; i++) rr = __dadd_rn(rr, fR[i]);
+#pragma unroll
+        for (int i = 0; i < NV; i++) rb = __dadd_rn(rb, fB[i]);
+        const long long o = (long long)y * c.pitch + x;
+        double vx, vy, vz;
+        if (form == ITLBM_FIELDS_VTK) {
+            double m[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+            sfor<0, NV>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                if constexpr (cx(i) != 0) {
+                    m[0][0] = __dadd_rn(m[0][0], cx(i) > 0 ? fR[i] : -fR[i]);
+                    m[1][0] = __dadd_rn(m[1][0], cx(i) > 0 ? fB[i] : -fB[i]);
+                }
+                if constexpr (cy(i) != 0) {
+                    m[0][1] = __dadd_rn(m[0][1], cy(i) > 0 ? fR[i] : -fR[i]);
+                    m[1][1] = __dadd_rn(m[1][1], cy(i) > 0 ? fB[i] : -fB[i]);
+                }
+                if constexpr (cz(i) != 0) {
+                    m[0][2] = __dadd_rn(m[0][2], cz(i) > 0 ? fR[i] : -fR[i]);
+                    m[1][2] = __dadd_rn(m[1][2], cz(i) > 0 ? fB[i] : -fB[i]);
+                }
+            });
+            double v[2][3];
+            const double rc[2] = {rr, rb};
+            for (int k = 0; k < 2; k++) {
+                if (rc[k] != 0.0) {
+                    const double inv = 1.0 / rc[k];
+                    for (int a = 0; a < 3; a++) v[k][a] = __dmul_rn(m[k][a], inv);
+                } else {
+                    for (int a = 0; a < 3; a++) v[k][a] = 0.0;
+                }
+            }
+            const double concR = rr / __dadd_rn(rr, rb);
+            const double concB = __dsub_rn(1.0, concR);
+            vx = __dadd_rn(__dmul_rn(concR, v[0][0]), __dmul_rn(concB, v[1][0]));
+            vy = __dadd_rn(__dmul_rn(concR, v[0][1]), __dmul_rn(concB, v[1][1]));
+            vz = __dadd_rn(__dmul_rn(concR, v[0][2]), __dmul_rn(concB, v[1][2]));
+            const double rho = __dadd_rn(rr, rb);
+            if (use_force && rho > 0.0) {
+                vx = __dsub_rn(vx, __dmul_rn(0.5, c.aux[o]) / rho);
+                vy = __dsub_rn(vy, __dmul_rn(0.5, c.aux[c.stride + o]) / rho);
+                vz = __dsub_rn(vz, __dmul_rn(0.5, c.aux[2 * c.stride + o]) / rho);
+            }
+        } else {
+            double jx = 0.0, jy = 0.0, jz = 0.0;
+            sfor<0, NV>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                const double f = __dadd_rn(fR[i], fB[i]);
+                if constexpr (cx(i) != 0) jx = __dadd_rn(jx, cx(i) > 0 ? f : -f);
+                if constexpr (cy(i) != 0) jy = __dadd_rn(jy, cy(i) > 0 ? f : -f);
+                if constexpr (cz(i) != 0) jz = __dadd_rn(jz, cz(i) > 0 ? f : -f);
+            });
+            const double rho = __dadd_rn(rr, rb);
+            if (!(rho > 0)) {
+                vx = vy = vz = CUDART_NAN;
+            } else {
+                if (use_force) {
+                    jx = __dsub_rn(jx, __dmul_rn(0.5, c.aux[o]));
+                    jy = __dsub_rn(jy, __dmul_rn(0.5, c.aux[c.stride + o]));
+                    jz = __dsub_rn(jz, __dmul_rn(0.5, c.aux[2 * c.stride + o]));
+                }
+                vx = jx / rho;
+                vy = jy / rho;
+                vz = jz / rho;
+            }
         }
         if (rR_out) rR_out[p] = rr;
         if (rB_out) rB_out[p] = rb;
-        if (ux_out) ux_out[p] = mx / rho;
-        if (uy_out) uy_out[p] = my / rho;
-        if (uz_out) uz_out[p] = mz / rho;
+        if (ux_out) ux_out[p] = vx;
+        if (uy_out) uy_out[p] = vy;
+        if (uz_out) uz_out[p] = vz;
     }
 }
 
@@ -866,109 +1054,157 @@ int nblocks_for(long long n) {
     return (int)(b < 1 ? 1 : b);
 }
 
-}  // namespace
-
-cudaError_t diag_alloc(DiagScratch &s, int nx, int ny) {
-    const int n = nx * ny;
-    const int nshell = (int)(sqrt((double)(nx * nx + ny * ny + 1)) / 0.5) + 2;
-    if (s.node && s.n == n && s.nshell == nshell) return cudaSuccess;
-    diag_free(s);
-    s.n = n;
-    s.nblocks = nblocks_for(n);
-    s.nshell = nshell;
-    cudaError_t e;
-    if ((e = cudaMalloc(&s.node, sizeof(double) * 6 * (size_t)n)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&s.part, sizeof(double) * 32 * (size_t)MAXB)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&s.shell, sizeof(long long) * 2 * (size_t)nshell)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&s.state, sizeof(DropState) + sizeof(StripState) + 64)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&s.out, sizeof(itlbm_drop_diag) + sizeof(itlbm_strip_diag) + 64)) != cudaSuccess)
-        return e;
-    return cudaSuccess;
-}
-
-namespace {
 size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
 int nshell_for(int nx, int ny) { return (int)(sqrt((double)(nx * nx + ny * ny + 1)) / 0.5) + 2; }
+constexpr size_t STATE_BYTES = sizeof(DropState) > sizeof(StripState) ? sizeof(DropState) : sizeof(StripState);
+constexpr size_t OUT_BYTES =
+    sizeof(itlbm_drop_diag) > sizeof(itlbm_strip_diag) ? sizeof(itlbm_drop_diag) : sizeof(itlbm_strip_diag);
+constexpr int PART_COLS = 32;  // >= the quantities of any pass
+static_assert(A_Q <= PART_COLS && B_Q <= PART_COLS && S_Q <= PART_COLS, "partial rows");
+
+cudaError_t run_drop(const DiagJob *jobs, int njobs, const int *blk_job, int total_blocks, const DiagJob &one,
+                     cudaStream_t st) {
+    const int g32 = (njobs + 31) / 32;
+    k_drop_clear<<<njobs, DT, 0, st>>>(jobs, one);
+    k_drop_d1<<<total_blocks, DT, 0, st>>>(jobs, blk_job, one);
+    k_reduce_jobs<A_Q, A_NS, A_NM, R_DROP_A><<<njobs, DT, 0, st>>>(jobs, one);
+    k_drop_f1<<<g32, 32, 0, st>>>(jobs, njobs, one);
+    k_drop_d2<<<total_blocks, DT, 0, st>>>(jobs, blk_job, one);
+    k_reduce_jobs<B_Q, B_NS, B_NM, R_DROP_B><<<njobs, DT, 0, st>>>(jobs, one);
+    k_drop_f2<<<g32, 32, 0, st>>>(jobs, njobs, one);
+    k_drop_fit<<<njobs, DT, 0, st>>>(jobs, one);
+    k_drop_modes<<<njobs * MODE_BLOCKS, DT, 0, st>>>(jobs, one);
+    k_drop_modes_sum<<<njobs, ITLBM_N_ANG, 0, st>>>(jobs, one);
+    return cudaGetLastError();
+}
+
+cudaError_t run_strip(const DiagJob *jobs, int njobs, const int *blk_job, int total_blocks, const DiagJob &one,
+                      cudaStream_t st) {
+    const int g32 = (njobs + 31) / 32;
+    k_strip_clear<<<njobs, DT, 0, st>>>(jobs, one);
+    k_strip_s1<<<total_blocks, DT, 0, st>>>(jobs, blk_job, one);
+    k_reduce_jobs<S_Q, S_NS, S_NM, R_STRIP_A><<<njobs, DT, 0, st>>>(jobs, one);
+    k_strip_f1<<<g32, 32, 0, st>>>(jobs, njobs, one);
+    k_strip_s2<<<total_blocks, DT, 0, st>>>(jobs, blk_job, one);
+    k_reduce_jobs<1, 0, 1, R_STRIP_RES><<<njobs, DT, 0, st>>>(jobs, one);
+    k_strip_f2<<<g32, 32, 0, st>>>(jobs, njobs, one);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
-size_t diag_bytes(int nx, int ny) {
+int diag_nblocks(long long n) { return nblocks_for(n); }
+
+size_t diag_job_bytes(int nx, int ny, int geometry) {
     const size_t n = (size_t)nx * ny;
-    return up256(sizeof(double) * 6 * n) + up256(sizeof(double) * 32 * (size_t)MAXB) +
-           up256(sizeof(long long) * 2 * (size_t)nshell_for(nx, ny)) +
-           up256(sizeof(DropState) + sizeof(StripState) + 64) +
-           up256(sizeof(itlbm_drop_diag) + sizeof(itlbm_strip_diag) + 64);
+    size_t b = up256(STATE_BYTES) + up256(OUT_BYTES) + up256(sizeof(double) * PART_COLS * nblocks_for((long long)n));
+    if (geometry == ITLBM_GEOM_DROP)
+        b += up256(sizeof(double) * 6 * n) + up256(sizeof(unsigned long long) * 2 * (size_t)nshell_for(nx, ny)) +
+             up256(sizeof(double) * 7 * ITLBM_N_ANG);
+    return b;
+}
+
+void diag_job_layout(DiagJob &j, void *base, int nx, int ny, int geometry) {
+    const size_t n = (size_t)nx * ny;
+    char *p = (char *)base;
+    j.n = (int)n;
+    j.nblocks = nblocks_for((long long)n);
+    j.nshell = geometry == ITLBM_GEOM_DROP ? nshell_for(nx, ny) : 0;
+    j.state = p;
+    p += up256(STATE_BYTES);
+    j.out = p;
+    p += up256(OUT_BYTES);
+    j.part = (double *)p;
+    p += up256(sizeof(double) * PART_COLS * j.nblocks);
+    j.node = nullptr;
+    j.shell = nullptr;
+    j.rays = nullptr;
+    if (geometry == ITLBM_GEOM_DROP) {
+        j.node = (double *)p;
+        p += up256(sizeof(double) * 6 * n);
+        j.shell = (unsigned long long *)p;
+        p += up256(sizeof(unsigned long long) * 2 * (size_t)j.nshell);
+        j.rays = (double *)p;
+    }
+    j.block0 = 0;
+}
+
+cudaError_t launch_diag_jobs(const DiagJob *jobs_dev, int njobs, const int *blk_job, int total_blocks,
+                             int geometry, cudaStream_t st) {
+    if (njobs <= 0) return cudaSuccess;
+    const DiagJob none{};
+    return geometry == ITLBM_GEOM_DROP ? run_drop(jobs_dev, njobs, blk_job, total_blocks, none, st)
+                                       : run_strip(jobs_dev, njobs, blk_job, total_blocks, none, st);
+}
+
+size_t diag_bytes(int nx, int ny) { return diag_job_bytes(nx, ny, ITLBM_GEOM_DROP); }
+
+void *diag_scratch_out(const DiagScratch &s) { return s.base ? (char *)s.base + up256(STATE_BYTES) : nullptr; }
+
+cudaError_t diag_alloc(DiagScratch &s, int nx, int ny) {
+    const size_t need = diag_bytes(nx, ny);
+    if (s.base && s.bytes >= need) return cudaSuccess;
+    diag_free(s);
+    void *p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) return e;  // s stays empty: the next call tries again
+    s.base = p;
+    s.bytes = need;
+    s.owned = true;
+    return cudaSuccess;
 }
 
 cudaError_t diag_bind(DiagScratch &s, void *base, size_t bytes, int nx, int ny) {
     if (!base || ((uintptr_t)base & 255) || diag_bytes(nx, ny) > bytes) return cudaErrorInvalidValue;
-    const int n = nx * ny;
-    char *p = (char *)base;
-    s.n = n;
-    s.nblocks = nblocks_for(n);
-    s.nshell = nshell_for(nx, ny);
-    s.node = (double *)p;
-    p += up256(sizeof(double) * 6 * (size_t)n);
-    s.part = (double *)p;
-    p += up256(sizeof(double) * 32 * (size_t)MAXB);
-    s.shell = (long long *)p;
-    p += up256(sizeof(long long) * 2 * (size_t)s.nshell);
-    s.state = (double *)p;
-    p += up256(sizeof(DropState) + sizeof(StripState) + 64);
-    s.out = p;
+    s.base = base;
+    s.bytes = bytes;
+    s.owned = false;
     return cudaSuccess;
 }
 
 void diag_free(DiagScratch &s) {
-    if (s.node) cudaFree(s.node);
-    if (s.part) cudaFree(s.part);
-    if (s.shell) cudaFree(s.shell);
-    if (s.state) cudaFree(s.state);
-    if (s.out) cudaFree(s.out);
+    if (s.owned && s.base) cudaFree(s.base);
     s = DiagScratch();
 }
 
 cudaError_t launch_diag_drop(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
                              int step, double v0, double x_ini, double y_ini, bool use_force,
                              itlbm_drop_diag *out_dev, cudaStream_t st) {
-    DropState *ds = (DropState *)s.state;
-    const int nb = s.nblocks;
-    cudaMemsetAsync(out_dev, 0, sizeof(itlbm_drop_diag), st);
-    cudaMemsetAsync(s.shell, 0, sizeof(long long) * 2 * (size_t)s.nshell, st);
-    k_drop_d1<<<nb, DT, 0, st>>>(c_dev, cur, use_force ? 1 : 0, s.node, s.part);
-    k_reduce<A_Q, A_NS, A_NM><<<1, DT, 0, st>>>(s.part, nb, ds->a);
-    k_drop_f1<<<1, 1, 0, st>>>(c_dev, ds, out_dev);
-    k_drop_d2<<<nb, DT, 0, st>>>(c_dev, ds, out_dev, v0, s.node, s.part,
-                                 (unsigned long long *)s.shell, s.nshell);
-    k_reduce<B_Q, B_NS, B_NM><<<1, DT, 0, st>>>(s.part, nb, ds->b);
-    k_drop_f2<<<1, 1, 0, st>>>(c_dev, ds, out_dev, step, v0, x_ini, y_ini, s.node);
-    k_drop_fit<<<1, DT, 0, st>>>(ds, out_dev, (const unsigned long long *)s.shell, s.nshell);
-    k_drop_modes<<<1, ITLBM_N_ANG, 0, st>>>(c_dev, ds, out_dev, s.node);
-    (void)c;
-    return cudaGetLastError();
+    if (!s.base || s.bytes < diag_bytes(c.nx, c.ny)) return cudaErrorInvalidValue;
+    DiagJob j{};
+    diag_job_layout(j, s.base, c.nx, c.ny, ITLBM_GEOM_DROP);
+    j.c = c_dev;
+    if (out_dev) j.out = out_dev;
+    j.cur = cur;
+    j.step = step;
+    j.v0 = v0;
+    j.x_ini = x_ini;
+    j.y_ini = y_ini;
+    j.use_force = use_force ? 1 : 0;
+    return run_drop(nullptr, 1, nullptr, j.nblocks, j, st);
 }
 
 cudaError_t launch_diag_strip(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
                               int step, int p, int q, bool use_force, itlbm_strip_diag *out_dev,
                               cudaStream_t st) {
-    StripState *ss = (StripState *)((char *)s.state + sizeof(DropState));
-    const int nb = s.nblocks;
-    cudaMemsetAsync(out_dev, 0, sizeof(itlbm_strip_diag), st);
-    k_strip_s1<<<nb, DT, 0, st>>>(c_dev, cur, p, q, use_force ? 1 : 0, s.part);
-    k_reduce<S_Q, S_NS, S_NM><<<1, DT, 0, st>>>(s.part, nb, ss->a);
-    k_strip_f1<<<1, 1, 0, st>>>(c_dev, ss, p, q, out_dev);
-    k_strip_s2<<<nb, DT, 0, st>>>(c_dev, cur, p, q, ss, s.part);
-    k_reduce<1, 0, 1><<<1, DT, 0, st>>>(s.part, nb, ss->res);
-    k_strip_f2<<<1, 1, 0, st>>>(ss, out_dev);
-    (void)c;
-    (void)step;
-    return cudaGetLastError();
+    if (!s.base || s.bytes < diag_job_bytes(c.nx, c.ny, ITLBM_GEOM_STRIP)) return cudaErrorInvalidValue;
+    DiagJob j{};
+    diag_job_layout(j, s.base, c.nx, c.ny, ITLBM_GEOM_STRIP);
+    j.c = c_dev;
+    if (out_dev) j.out = out_dev;
+    j.cur = cur;
+    j.step = step;
+    j.p = p;
+    j.q = q;
+    j.use_force = use_force ? 1 : 0;
+    return run_strip(nullptr, 1, nullptr, j.nblocks, j, st);
 }
 
-cudaError_t launch_fields(const CaseDev *c_dev, const CaseDev &c, int cur, bool use_force,
+cudaError_t launch_fields(const CaseDev *c_dev, const CaseDev &c, int cur, bool use_force, int form,
                           double *rho_R, double *rho_B, double *ux, double *uy, double *uz,
                           cudaStream_t st) {
     const long long n = (long long)c.nx * c.ny;
-    k_fields<<<nblocks_for(n), DT, 0, st>>>(c_dev, cur, use_force ? 1 : 0, rho_R, rho_B, ux, uy, uz);
+    k_fields<<<nblocks_for(n), DT, 0, st>>>(c_dev, cur, use_force ? 1 : 0, form, rho_R, rho_B, ux, uy, uz);
     return cudaGetLastError();
 }
 

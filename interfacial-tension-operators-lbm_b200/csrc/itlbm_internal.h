@@ -180,32 +180,62 @@ cudaError_t launch_export(const CaseDev *c_dev, int nx, int ny, int cur, int whi
 cudaError_t launch_import(const CaseDev *c_dev, int nx, int ny, int cur, const double *fR,
                           const double *fB, cudaStream_t s);
 
-// Diagnostic scratch (per case, allocated on demand).
-struct DiagScratch {
-    double *node = nullptr;      // per node: rho_R, rho_B, ux, uy, uz, phi (6 arrays of n)
-    double *part = nullptr;      // per-block partial sums
-    long long *shell = nullptr;  // shell histogram (fixed point) and counts
-    double *state = nullptr;     // device-side running state of one diagnostic
-    void *out = nullptr;         // device copy of the output struct
-    int n = 0, nblocks = 0, nshell = 0;
+// One diagnostic of one case: where its case descriptor, its scratch and its result are, and what
+// to measure.  The drop and strip diagnostics of any number of cases run as one sequence of launches
+// over a table of these (itlbm_batch.cu), or of a single one passed by value (a single case).  Every
+// case keeps the reduction order it has alone -- its own number of partial blocks, visited in the
+// same order -- so a case gives the same bits alone and in a batch.
+struct DiagJob {
+    const CaseDev *c;             // the case descriptor (device memory)
+    double *node;                 // drop: per node rho_R, rho_B, ux, uy, uz, phi (6 arrays of n)
+    double *part;                 // per-block partials, nblocks rows
+    unsigned long long *shell;    // drop: shell histogram (fixed point) and counts, 2 x nshell
+    void *state;                  // running state of the diagnostic
+    void *out;                    // itlbm_drop_diag or itlbm_strip_diag (device memory)
+    double *rays;                 // drop: the harmonic products of the 256 rays, 7 x 256
+    double v0, x_ini, y_ini;
+    int cur, step, use_force;
+    int n, nblocks, nshell;       // nodes, partial blocks and shells of the case
+    int block0;                   // first block of this job in the grids of the full-field passes
+    int p, q;                     // strip normal
 };
-cudaError_t diag_alloc(DiagScratch &s, int nx, int ny);
+// Layout of one job's scratch: bytes needed for an nx x ny case (a drop needs more than a strip), and
+// the job's pointers laid out in a 256-byte aligned block of at least that many bytes.
+size_t diag_job_bytes(int nx, int ny, int geometry);
+void diag_job_layout(DiagJob &j, void *base, int nx, int ny, int geometry);
+// Partial blocks of a full-field pass over n nodes (part of the reduction order of a case).
+int diag_nblocks(long long n);
+// A diagnostic of every job of a table on one stream: jobs_dev[njobs], all of one geometry, with the
+// full-field passes over total_blocks blocks, blk_job[b] the job of block b.
+cudaError_t launch_diag_jobs(const DiagJob *jobs_dev, int njobs, const int *blk_job, int total_blocks,
+                             int geometry, cudaStream_t st);
+
+// Diagnostic scratch of a single case, allocated on demand (or bound to a block the caller holds).
+struct DiagScratch {
+    void *base = nullptr;
+    size_t bytes = 0;
+    bool owned = false;
+};
+cudaError_t diag_alloc(DiagScratch &s, int nx, int ny);  // on failure s is left empty
 void diag_free(DiagScratch &s);
 // Bytes of one diagnostic scratch for an nx x ny case, and the same scratch laid out in a block the
 // caller already holds (256-byte aligned, at least diag_bytes long); diag_bind allocates nothing and
-// the block stays the caller's (never pass a bound scratch to diag_free).
+// the block stays the caller's (diag_free leaves a bound block alone).
 size_t diag_bytes(int nx, int ny);
 cudaError_t diag_bind(DiagScratch &s, void *base, size_t bytes, int nx, int ny);
+// Where a diagnostic on this scratch leaves its result when launched with out_dev == nullptr.
+void *diag_scratch_out(const DiagScratch &s);
 // The static scratch of itlbm_case_diag_drop_static on the current device: its address (looked up
 // once per device) and its size in bytes.
 cudaError_t static_diag_scratch(int device, void **base, size_t *bytes);
+// One diagnostic of a single case on its scratch; out_dev receives the result (device memory).
 cudaError_t launch_diag_drop(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
                              int step, double v0, double x_ini, double y_ini, bool use_force,
                              itlbm_drop_diag *out_dev, cudaStream_t st);
 cudaError_t launch_diag_strip(const CaseDev *c_dev, const CaseDev &c, DiagScratch &s, int cur,
                               int step, int p, int q, bool use_force, itlbm_strip_diag *out_dev,
                               cudaStream_t st);
-cudaError_t launch_fields(const CaseDev *c_dev, const CaseDev &c, int cur, bool use_force,
+cudaError_t launch_fields(const CaseDev *c_dev, const CaseDev &c, int cur, bool use_force, int form,
                           double *rho_R, double *rho_B, double *ux, double *uy, double *uz,
                           cudaStream_t st);
 
@@ -225,5 +255,7 @@ int snap_read_state(const char *path, const CaseDev &h, void *state);
 void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
+// cudaSetDevice with its return checked: ITLBM_OK or the failure, with the message set.
+int use_device(int device);
 
 }  // namespace itlbm

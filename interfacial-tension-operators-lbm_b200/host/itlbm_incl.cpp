@@ -117,8 +117,8 @@ int main(int argc, char **argv) {
             if (ultimo) {  // perfil.dat, Imm_INCL.cpp:101, :162
                 const size_t n = (size_t)N * N;
                 std::vector<double> rR(n), rB(n), ux(n), uy(n);
-                if (itlbm_case_read_fields(c, rR.data(), rB.data(), ux.data(), uy.data(), nullptr, nullptr) != ITLBM_OK)
-                    return die(c, 2, "itlbm_case_read_fields");
+                if (itlbm_case_read_profile(c, rR.data(), rB.data(), ux.data(), uy.data()) != ITLBM_OK)
+                    return die(c, 2, "itlbm_case_read_profile");
                 write_perfil(join(dir, "perfil.dat"), N, p, q, rR, rB, ux, uy);
             }
             if (run.on_diag(step, r, &std::cout)) break;

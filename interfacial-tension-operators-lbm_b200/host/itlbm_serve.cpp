@@ -23,8 +23,13 @@
 //     diagnostic history in estado_itlbm.run) at every diagnostic; a request for a folder holding a
 //     snapshot of the same case short of its step count resumes from it instead of step 0 (the
 //     reference restarts from step 0, rodar_lote.py:5-7), with the same results.
+//   * a drop that finishes gets its final fields, rho_R<n>.vtk, rho_B<n>.vtk and vel_<n>.vtk at its
+//     last step n (Imm_OPS.cpp:357-364; an unstable run stops before them), a strip that reaches its
+//     last step gets perfil.dat (Imm_INCL.cpp:101, :162): the batch holds a retired case's state until
+//     they are written;
 // The client bin/itlbm_submit turns this into a drop-in for the Imm_OPS binary of rodar_lote.py.
-// The final VTK fields and perfil.dat are written only by itlbm_ops / itlbm_incl.
+// Fields at intermediate steps (data_in.txt `files` > 0; rodar_lote.py writes 0) are written by
+// itlbm_ops only.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -245,6 +250,7 @@ int main(int argc, char **argv) {
         std::cerr << "itlbm_batch_create: " << itlbm_last_error() << std::endl;
         return 2;
     }
+    itlbm_batch_hold_finished(b, 1);  // retired cases wait for their final fields
     std::map<long long, Job> jobs;
     long long next_tag = 0;
     std::vector<double> latencies;
@@ -323,6 +329,34 @@ int main(int argc, char **argv) {
                     }
                     continue;
                 }
+                // final fields, read from the held state, then the case's memory goes back to the batch
+                const int last = j.n_steps - 1;
+                const size_t n = (size_t)j.desc.nx * j.desc.ny;
+                if (j.drop && e.kind == ITLBM_EV_DONE) {
+                    std::vector<double> rR(n), rB(n), ux(n), uy(n), uz(n);
+                    if (itlbm_batch_read_fields(b, e.tag, ITLBM_FIELDS_VTK, rR.data(), rB.data(), ux.data(), uy.data(),
+                                                uz.data()) == ITLBM_OK) {
+                        const std::string sfx = std::to_string((unsigned)last);
+                        write_vtk_scalar(join(j.dir, "rho_R" + sfx + ".vtk"), "Densidade", "densidade", j.desc.nx,
+                                         j.desc.ny, rR.data());
+                        write_vtk_scalar(join(j.dir, "rho_B" + sfx + ".vtk"), "Densidade", "densidade", j.desc.nx,
+                                         j.desc.ny, rB.data());
+                        write_vtk_velocity(join(j.dir, "vel_" + sfx + ".vtk"), j.desc.nx, j.desc.ny, ux.data(),
+                                           uy.data(), uz.data());
+                    } else {
+                        std::cerr << "itlbm_serve: no final fields for " << j.dir << ": " << itlbm_last_error()
+                                  << std::endl;
+                    }
+                } else if (!j.drop && (e.kind == ITLBM_EV_DONE || e.step == last)) {
+                    std::vector<double> rR(n), rB(n), ux(n), uy(n);
+                    if (itlbm_batch_read_fields(b, e.tag, ITLBM_FIELDS_PROFILE, rR.data(), rB.data(), ux.data(),
+                                                uy.data(), nullptr) == ITLBM_OK)
+                        write_perfil(join(j.dir, "perfil.dat"), j.desc.nx, j.desc.p, j.desc.q, rR, rB, ux, uy);
+                    else
+                        std::cerr << "itlbm_serve: no perfil.dat for " << j.dir << ": " << itlbm_last_error()
+                                  << std::endl;
+                }
+                itlbm_batch_release(b, e.tag);
                 const double t = now_s(), latency = t - j.t_submit;
                 const int steps = e.step;
                 const double mlups = latency > 0 ? (double)j.desc.nx * j.desc.ny * steps / (latency * 1e6) : 0;

@@ -1064,3 +1064,68 @@ int orc_diag_strip(orc_case *c, int step, int p, int q, itlbm_strip_diag *r) {
     r->ok = (r->n_ruim == 0 && isfin(r->u_max));
     return r->ok;
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* per-node output fields of the post-collision populations of the last step                  */
+/* ------------------------------------------------------------------------------------------ */
+
+/* form ITLBM_FIELDS_VTK: rec_density (LBM_functions.cpp:1457-1511) -- rho_R, rho_B by density() --
+ * and rec_velocity's two-colour branch (:1349-1458): the colour velocities by calcula, weighted by the
+ * concentrations, minus (F/2)/rho when the program keeps a force (class F, Imm_OPS.cpp:171-181).
+ * form ITLBM_FIELDS_PROFILE: the columns of perfil.dat in mede_inclinada (Imm_INCL.cpp:104-162):
+ * u = (sum_i f_i c_i - F/2) / rho with f_i = f_R,i + f_B,i; nodes with !(rho > 0) get no velocity
+ * there (they are skipped), and NaN here. */
+void orc_fields(const orc_case *c, int form, double *rho_R, double *rho_B, double *ux, double *uy,
+                double *uz) {
+    const double *forca = (c->tipo >= ITLBM_OP_F1) ? c->force : NULL;
+    for (int p = 0; p < c->n; p++) {
+        const double *fR = c->fR_post + (size_t)p * NV, *fB = c->fB_post + (size_t)p * NV;
+        double rR = density(fR), rB = density(fB);
+        double vx, vy, vz;
+        if (form == ITLBM_FIELDS_VTK) {
+            double vxR, vyR, vzR, rhoR, vxB, vyB, vzB, rhoB;
+            calcula(fR, &vxR, &vyR, &vzR, &rhoR);
+            calcula(fB, &vxB, &vyB, &vzB, &rhoB);
+            double concR = rhoR / (rhoR + rhoB);
+            double concB = 1. - concR;
+            vx = concR * vxR + concB * vxB;
+            vy = concR * vyR + concB * vyB;
+            vz = concR * vzR + concB * vzB;
+            if (forca) {
+                double rho = rhoR + rhoB;
+                const double *F = forca + 3 * (size_t)p;
+                if (rho > 0.0) {
+                    vx = vx - 0.5 * F[0] / rho;
+                    vy = vy - 0.5 * F[1] / rho;
+                    vz = vz - 0.5 * F[2] / rho;
+                }
+            }
+        } else {
+            double jx = 0, jy = 0, jz = 0;
+            for (int i = 0; i < NV; i++) {
+                double f = fR[i] + fB[i];
+                jx += f * CI[i][0];
+                jy += f * CI[i][1];
+                jz += f * CI[i][2];
+            }
+            double rho = rR + rB;
+            if (!(rho > 0)) {
+                vx = vy = vz = NAN;
+            } else {
+                if (forca) {
+                    jx -= 0.5 * forca[3 * (size_t)p];
+                    jy -= 0.5 * forca[3 * (size_t)p + 1];
+                    jz -= 0.5 * forca[3 * (size_t)p + 2];
+                }
+                vx = jx / rho;
+                vy = jy / rho;
+                vz = jz / rho;
+            }
+        }
+        if (rho_R) rho_R[p] = rR;
+        if (rho_B) rho_B[p] = rB;
+        if (ux) ux[p] = vx;
+        if (uy) uy[p] = vy;
+        if (uz) uz[p] = vz;
+    }
+}

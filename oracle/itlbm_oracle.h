@@ -44,6 +44,11 @@ int orc_diag_drop(orc_case *c, int step, double v0, double x_ini, double y_ini,
                   itlbm_drop_diag *out);
 int orc_diag_strip(orc_case *c, int step, int p, int q, itlbm_strip_diag *out);
 
+/* per-node output fields of the post-collision populations of the last step; form is
+ * ITLBM_FIELDS_VTK (rec_density / rec_velocity) or ITLBM_FIELDS_PROFILE (perfil.dat columns) */
+void orc_fields(const orc_case *c, int form, double *rho_R, double *rho_B, double *ux, double *uy,
+                double *uz);
+
 /* per-site operator functions (E0 checks) */
 void orc_perturbacao(int tipo, double chi, double A, const double *g, double *f);
 void orc_source(const double *F, const double *u, double rho, double tau, double *S);

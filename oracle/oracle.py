@@ -70,6 +70,7 @@ def orc():
             "orc_source": (None, [_dp, _dp, d, d, _dp]),
             "orc_calcula_forca": (None, [i, d, d, i, i, _dp, _dp, _dp]),
             "orc_colisao_comum": (None, [i, d, d, d, d, _dp, _dp, _dp, _dp]),
+            "orc_fields": (None, [vp, i, _dp, _dp, _dp, _dp, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -123,6 +124,13 @@ class OracleCase:
 
     def step(self, n=1):
         orc().orc_step(self._h, int(n))
+
+    def fields(self, form=0):
+        """rec_density / rec_velocity (form 0) or the perfil.dat columns (form 1) of the post-collision
+        populations of the last step."""
+        out = {k: np.empty(self.n) for k in ("rho_R", "rho_B", "ux", "uy", "uz")}
+        orc().orc_fields(self._h, int(form), *[_ptr(out[k]) for k in ("rho_R", "rho_B", "ux", "uy", "uz")])
+        return out
 
     def diag_drop(self, step, v0=0.0, x_ini=None, y_ini=None):
         d = DropDiag()
@@ -192,6 +200,7 @@ def _load_ref():
             ("ref_ops_get_pops", None, [vp, i, _dp, _dp]),
             ("ref_ops_get_force", None, [vp, _dp]),
             ("ref_ops_diag", i, [vp, i, d, d, d, _P(DropDiag)]),
+            ("ref_ops_write_fields", i, [vp, i, C.c_char_p]),
             ("ref_ops_destroy", None, [vp]),
         ]:
             f = getattr(L, name)
@@ -203,6 +212,7 @@ def _load_ref():
             ("ref_incl_step", None, [vp, i]),
             ("ref_incl_get_pops", None, [vp, i, _dp, _dp]),
             ("ref_incl_diag", i, [vp, i, _P(StripDiag)]),
+            ("ref_incl_write_perfil", i, [vp, C.c_char_p]),
             ("ref_incl_destroy", None, [vp]),
         ]:
             f = getattr(L2, name)
@@ -245,6 +255,12 @@ class RefDrop:
         _ref_ops.ref_ops_diag(self._h, step, v0, float(x_ini), float(y_ini), C.byref(d))
         return d
 
+    def write_fields(self, step, directory):
+        """rho_R<step>.vtk, rho_B<step>.vtk and vel_<step>.vtk of the post-collision populations, written
+        into `directory` by the reference's rec_density / rec_velocity."""
+        if not _ref_ops.ref_ops_write_fields(self._h, int(step), str(directory).encode()):
+            raise RuntimeError(f"cannot write the fields into {directory}")
+
     def close(self):
         if self._h:
             _ref_ops.ref_ops_destroy(self._h)
@@ -277,6 +293,11 @@ class RefStrip:
         d = StripDiag()
         _ref_incl.ref_incl_diag(self._h, step, C.byref(d))
         return d
+
+    def write_perfil(self, directory):
+        """perfil.dat of the post-collision populations, written into `directory` by mede_inclinada."""
+        if not _ref_incl.ref_incl_write_perfil(self._h, str(directory).encode()):
+            raise RuntimeError(f"cannot write perfil.dat into {directory}")
 
     def close(self):
         if self._h:
@@ -320,6 +341,36 @@ class RefStepper:
     def close(self):
         if self._h:
             self._L.ref_ops_destroy(self._h)
+            self._h = None
+
+
+class RefStripStepper:
+    """The reference's own Imm_INCL step loop (Imm_INCL.cpp:358-442) on one inclined-strip case, through
+    oracle/_ref/libref_incl_fast.so (the reference's own flags), on `threads` host threads (0 = all
+    cores).  A CPU baseline, never a product path."""
+
+    def __init__(self, N, tipo=3, p=1, q=0, chi=0.5, xi=1.569988, tau=1.0, beta=0.8, A=0.225, threads=0):
+        import os
+        L = C.CDLL(str(REF_DIR / "libref_incl_fast.so"))
+        vp, d, i = C.c_void_p, C.c_double, C.c_int
+        L.ref_incl_create.restype, L.ref_incl_create.argtypes = vp, [i, i, d, d, d, d, d, i, i, i]
+        L.ref_incl_step.restype, L.ref_incl_step.argtypes = None, [vp, i]
+        L.ref_incl_destroy.restype, L.ref_incl_destroy.argtypes = None, [vp]
+        self._L = L
+        self.threads = threads if threads > 0 else (os.cpu_count() or 1)
+        self.nodes = N * N
+        self._h = L.ref_incl_create(N, tipo, chi, xi, tau, beta, A, p, q, self.threads)
+
+    def step(self, n):
+        """n steps; returns the wall time in seconds."""
+        import time
+        t0 = time.perf_counter()
+        self._L.ref_incl_step(self._h, n)
+        return time.perf_counter() - t0
+
+    def close(self):
+        if self._h:
+            self._L.ref_incl_destroy(self._h)
             self._h = None
 
 

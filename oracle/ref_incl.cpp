@@ -9,6 +9,8 @@
 
 #include "../include/itlbm.h"
 
+#include <unistd.h>
+
 namespace {
 struct RefIncl {
     GEOMETRY geometry;
@@ -157,6 +159,20 @@ int ref_incl_diag(void *h, int step, itlbm_strip_diag *out) {
     out->neg_total = res.neg_total; out->neg_cor = res.neg_cor; out->n_ruim = res.n_ruim;
     out->n_ajuste = res.n_ajuste;
     return ok ? 1 : 0;
+}
+
+// mede_inclinada with gravar_perfil (Imm_INCL.cpp:404 at the last step): writes perfil.dat of the
+// post-collision populations of the last step into directory `dir`.
+int ref_incl_write_perfil(void *h, const char *dir) {
+    RefIncl *r = (RefIncl *)h;
+    LATTICE L = r->lattice;
+    std::swap(L.inif_R, L.inif_R_new);
+    std::swap(L.inif_B, L.inif_B_new);
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd)) || chdir(dir) != 0) return 0;
+    INCL res;
+    mede_inclinada(r->geometry, L, r->p, r->q, res, r->forca, true);
+    return chdir(cwd) == 0 ? 1 : 0;
 }
 
 void ref_incl_destroy(void *h) {

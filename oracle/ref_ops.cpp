@@ -12,6 +12,8 @@
 
 #include "../include/itlbm.h"
 
+#include <unistd.h>
+
 namespace {
 struct RefOps {
     GEOMETRY geometry;
@@ -186,6 +188,21 @@ int ref_ops_diag(void *h, int step, double v0, double x_ini, double y_ini, itlbm
     out->negative_total = gi.negative_total; out->negative_color = gi.negative_color; out->bad = gi.bad;
     out->R0 = md.R0; out->a2 = md.a2; out->a4 = md.a4; out->a8 = md.a8; out->rmin = md.rmin; out->rmax = md.rmax;
     return ok ? 1 : 0;
+}
+
+// The final-field writers of Imm_OPS.cpp:357-364 (rec_density, rec_velocity) on the post-collision
+// populations of the last step, run in directory `dir` (they write into the working directory).
+int ref_ops_write_fields(void *h, int step, const char *dir) {
+    RefOps *r = (RefOps *)h;
+    LATTICE L = r->lattice;
+    std::swap(L.inif_R, L.inif_R_new);
+    std::swap(L.inif_B, L.inif_B_new);
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd)) || chdir(dir) != 0) return 0;
+    rec_density("rho_R", r->geometry, L.inif_R, (unsigned int)step);
+    rec_density("rho_B", r->geometry, L.inif_B, (unsigned int)step);
+    rec_velocity(r->geometry, L, (unsigned int)step);
+    return chdir(cwd) == 0 ? 1 : 0;
 }
 
 void ref_ops_destroy(void *h) {

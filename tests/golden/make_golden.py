@@ -1,18 +1,22 @@
 #!/usr/bin/env python3
 """Extract golden vectors from the reference's shipped outputs into small committed fixtures.
 
-Run once in a container that has the reference project (default /root/reference):
+Run once in a container that has the reference project:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference project root>    (or set ITLBM_REFERENCE)
 
 It writes
   lotes_subset.json   inputs and the first diagnostic rows (steps 0, 500, 1000) of a selection of the
                       stored runs under Lotes/ -- laplace.dat, iso.dat and galilean.dat of Imm_OPS
                       cases, inclinada.dat of Imm_INCL cases -- plus each case's resumo.dat line;
-  e0_resultado.json   the numbers of E0_resultado.txt (the reference's analytic operator checks).
-Nothing here runs the reference; the files are parsed as text.
+  e0_resultado.json   the numbers of E0_resultado.txt (the reference's analytic operator checks);
+  analisar_e2.json    three stored Lotes/E2 folders (their resumo.dat and laplace.dat as text) with the
+                      rows the reference's own analisar_lote.coleta makes of them (the only part of this
+                      script that imports reference code: the batch-table rows of a Python reference).
+Apart from analisar_lote.py nothing here runs the reference; the files are parsed as text.
 """
 import argparse
+import os
 import json
 import re
 from pathlib import Path
@@ -54,8 +58,10 @@ def header(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ITLBM_REFERENCE"))
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give --ref <reference project root> or set ITLBM_REFERENCE")
     ref = Path(a.ref)
     cases = []
     for batch, folder in CASES:
@@ -102,7 +108,25 @@ def main():
         if line.strip():
             section = line.strip()
     (HERE / "e0_resultado.json").write_text(json.dumps(e0, indent=1))
-    print(f"{len(cases)} cases, {len(e0['checks'])} E0 checks, {len(e0['m4'])} M4 rows")
+    # analisar_lote.coleta on stored E2 folders: three folders of different operators
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("analisar_lote", ref / "analisar_lote.py")
+    al = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(al)
+    lotes = ref / "Lotes"
+    picked, seen = [], set()
+    for row in al.coleta(lotes, "E2"):
+        op = row["pasta"].split("/")[0]
+        if op in seen or op not in ("P3 chi=0.5", "F2", "P1"):
+            continue
+        seen.add(op)
+        d = lotes / "E2" / row["pasta"]
+        picked.append({"pasta": row["pasta"], "row": {k: (None if isinstance(v, float) and v != v else v)
+                                                      for k, v in row.items()},
+                       "resumo.dat": (d / "resumo.dat").read_text(), "laplace.dat": (d / "laplace.dat").read_text()})
+    (HERE / "analisar_e2.json").write_text(json.dumps(picked, indent=1))
+    print(f"{len(cases)} cases, {len(e0['checks'])} E0 checks, {len(e0['m4'])} M4 rows, "
+          f"{len(picked)} analisar_lote rows")
 
 
 if __name__ == "__main__":

@@ -166,3 +166,47 @@ def test_launch_shapes_agree(gpu):
     assert len(rows[0]) == 2 * len(cases)  # the diagnostics at steps 0 and 128
     assert rows[0] == rows[-1] == rows[4]
     assert modes[-1] == -1 and modes[4] == 4 and modes[0] in (-1, 0)
+
+
+def test_held_cases_give_their_final_fields(gpu):
+    """With hold_finished, a retired case keeps its state until released and its final fields equal
+    those of the same case run alone, bit for bit (both velocity forms); it is off the work
+    table, so the others advance as before, and its memory counts until release."""
+    mix = [(40, 12, 0.1, 0, 0, (1, 0), 501, 0.05), (36, 3, 0.225, 0, 1, (2, 1), 600, 0.0),
+           (44, 13, 0.1, 1, 0, (1, 0), 700, 0.1), (48, 11, 0.1, 0, 0, (1, 0), 1300, 0.0)]
+    descs = [mkdesc(gpu, nx, t, A=A, prec=pr, geometry=g, p=pq[0], q=pq[1], v0=v0)
+             for nx, t, A, pr, g, pq, _, v0 in mix]
+    alone = []
+    for d, m in zip(descs, mix):
+        with gpu.Case(d) as c:
+            c.step(m[6], keep_aux=True)
+            alone.append((c.read_fields(), c.read_profile()))
+    got = {}
+    with gpu.Batch(chunk=250) as b:
+        b.hold_finished(True)
+        for k, d in enumerate(descs):
+            b.submit(d, mix[k][6], k)
+        for _ in range(100):
+            b.advance()
+            for e in b.poll():
+                if e.kind == gpu.EV_DIAG:
+                    continue
+                assert e.kind == gpu.EV_DONE
+                n = descs[e.tag].nx * descs[e.tag].ny
+                used = b.stats().hbm_used
+                got[e.tag] = (b.read_fields(e.tag, n, gpu.FIELDS_VTK), b.read_fields(e.tag, n, gpu.FIELDS_PROFILE))
+                assert b.stats().held >= 1
+                b.release(e.tag)
+                assert b.stats().hbm_used < used
+                with pytest.raises(gpu.ItlbmError):
+                    b.release(e.tag)
+            st = b.stats()
+            if st.active == 0 and st.pending == 0 and st.held == 0:
+                break
+    assert sorted(got) == list(range(len(mix)))
+    for k, m in enumerate(mix):
+        (fa, pa), (fb, pb) = alone[k], got[k]
+        for key in ("rho_R", "rho_B", "ux", "uy", "uz"):
+            assert np.array_equal(fa[key], fb[key]), (k, key)
+        for key in ("rho_R", "rho_B", "ux", "uy"):
+            assert np.array_equal(pa[key], pb[key]), (k, key)

@@ -316,3 +316,45 @@ def test_invalid_descriptions_are_rejected(itlbm):
         with pytest.raises(itlbm.ItlbmError) as e:
             itlbm.Case(d)
         assert e.value.code == -1
+
+
+# ---- output fields (vel_*.vtk, rho_*.vtk, perfil.dat) -------------------------------------------
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS, ids=OP_IDS)
+def test_fields_bit_exact_drop(gpu, oracle, name, tipo, chi, xi, A):
+    """rec_density / rec_velocity (LBM_functions.cpp:1349-1511) and the perfil.dat velocity of a
+    translating drop: every value equal to the oracle's (which prints the reference's own VTK files
+    token for token, test_oracle_pin.py)."""
+    c = gpu_case(gpu, 37, 29, tipo, chi, xi, A, tau=0.7, radius=8.5, v0=0.1)
+    o = oracle.OracleCase(37, 29, tipo, chi, xi, tau=0.7, beta=0.8, A=A).init_drop(radius=8.5, v0=0.1)
+    c.step(120, keep_aux=True)
+    o.step(120)
+    g, r = c.read_fields(), o.fields(0)
+    for k in ("rho_R", "rho_B", "ux", "uy", "uz"):
+        assert np.array_equal(g[k], r[k]), (k, np.abs(g[k] - r[k]).max())
+    g, r = c.read_profile(), o.fields(1)
+    for k in ("rho_R", "rho_B", "ux", "uy"):
+        assert np.array_equal(g[k], r[k]), (k, np.abs(g[k] - r[k]).max())
+    c.close()
+
+
+@pytest.mark.parametrize("name,tipo,chi,xi,A", [OPS[1], OPS[4], OPS[5], OPS[6]], ids=[OP_IDS[i] for i in (1, 4, 5, 6)])
+def test_profile_bit_exact_strip(gpu, oracle, name, tipo, chi, xi, A):
+    c = gpu_case(gpu, 40, 40, tipo, chi, xi, A, tau=0.7, geometry=1, p=3, q=1)
+    o = oracle.OracleCase(40, 40, tipo, chi, xi, tau=0.7, beta=0.8, A=A).init_strip(3, 1)
+    c.step(90, keep_aux=True)
+    o.step(90)
+    g, r = c.read_profile(), o.fields(1)
+    for k in ("rho_R", "rho_B", "ux", "uy"):
+        assert np.array_equal(g[k], r[k]), (k, np.abs(g[k] - r[k]).max())
+    c.close()
+
+
+def test_fields_need_the_force_of_class_f(gpu):
+    c = gpu_case(gpu, 32, 32, 12, 0.5, 1.569988, 0.1)
+    c.step(3)
+    with pytest.raises(gpu.ItlbmError) as e:
+        c.read_profile()
+    assert e.value.code == -10
+    c.step(1, keep_aux=True)
+    assert np.isfinite(c.read_profile()["ux"]).all()
+    c.close()

@@ -1,7 +1,8 @@
 """Serving: bin/itlbm_serve batches case folders that arrive while others run; bin/itlbm_submit gives
 each request the process contract of Imm_OPS (the way rodar_lote.py runs it).  A case gives the same
 result served in the mix as run alone: in FP64 the served diagnostic files are byte-identical to
-those of bin/itlbm_ops on the same folder."""
+those of bin/itlbm_ops on the same folder, the final fields (rho_R / rho_B / vel_ VTK files of a
+drop, perfil.dat of a strip) included."""
 import os
 import subprocess
 import threading
@@ -56,8 +57,11 @@ def test_served_equals_alone_and_overlaps(tmp_path):
         prog = "itlbm_incl" if pq else "itlbm_ops"
         assert run(BIN / prog, alone).returncode == 0
         names = ["inclinada.dat"] if pq else ["laplace.dat", "iso.dat", "galilean.dat"]
+        # the final fields: perfil.dat of a strip (Imm_INCL.cpp:101, :162), the rho_R / rho_B / vel_
+        # files of a drop at its last step (Imm_OPS.cpp:357-364)
+        names += ["perfil.dat"] if pq else [f"rho_R{steps - 1}.vtk", f"rho_B{steps - 1}.vtk", f"vel_{steps - 1}.vtk"]
         for n in names:
-            assert (dirs[k] / n).read_text() == (alone / n).read_text(), (k, n)
+            assert (dirs[k] / n).read_bytes() == (alone / n).read_bytes(), (k, n)
         ra = (dirs[k] / "resumo.dat").read_text().splitlines()
         rb = (alone / "resumo.dat").read_text().splitlines()
         assert ra[0] == rb[0] and ra[1].split()[:-1] == rb[1].split()[:-1]  # all but the MLUPS column

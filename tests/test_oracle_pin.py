@@ -158,3 +158,66 @@ def test_oracle_reproduces_stored_strip_rows(oracle, itlbm, case):
             if step == 0 and name not in ("sigma_pop",):
                 tol = min(tol, 1e-8) if name not in ("u_max", "un_max", "ut_max", "res") else 1e-6
             assert _close(a, b, tol), (step, name, a, b)
+
+
+# ---- output fields -------------------------------------------------------------------------------
+def vtk_values(path):
+    """The numbers after the header of a STRUCTURED_POINTS file the reference writes, as text."""
+    lines = path.read_text().splitlines()
+    k = next(i for i, l in enumerate(lines) if l.startswith(("LOOKUP_TABLE", "VECTORS")))
+    return " ".join(lines[k + 1:]).split()
+
+
+def cxx(v):
+    """A double as `ostream << v` prints it with the default precision (%g with 6 digits)."""
+    return "%g" % v
+
+
+@needs_ref
+@pytest.mark.parametrize("name,tipo,chi,xi,A", OPS)
+def test_fields_match_reference_writers(oracle, tmp_path, name, tipo, chi, xi, A):
+    """rec_density / rec_velocity (LBM_functions.cpp:1349-1511): the oracle's fields printed as the
+    reference prints them give the reference's own rho_R / rho_B / vel_ files, token for token."""
+    nx, ny, v0 = 37, 29, 0.1
+    o = oracle.OracleCase(nx, ny, tipo, chi, xi, tau=0.7, beta=0.8, A=A).init_drop(radius=8.5, v0=v0)
+    r = oracle.RefDrop(nx, ny, tipo, chi, xi, tau=0.7, beta=0.8, A=A, radius=8.5, v0=v0, threads=1)
+    o.step(60)
+    r.step(60)
+    r.write_fields(59, tmp_path)
+    f = o.fields(0)
+    assert vtk_values(tmp_path / "rho_R59.vtk") == [cxx(v) for v in f["rho_R"]]
+    assert vtk_values(tmp_path / "rho_B59.vtk") == [cxx(v) for v in f["rho_B"]]
+    vel = np.stack([f["ux"], f["uy"], f["uz"]], axis=1).ravel()
+    assert vtk_values(tmp_path / "vel_59.vtk") == [cxx(v) for v in vel]
+
+
+@needs_ref
+@pytest.mark.parametrize("name,tipo,chi,xi,A", [OPS[2], OPS[4], OPS[5]])
+@pytest.mark.parametrize("N,p,q", [(40, 3, 1), (36, 1, 1)])
+def test_profile_matches_reference_perfil(oracle, tmp_path, name, tipo, chi, xi, A, N, p, q):
+    """perfil.dat (Imm_INCL.cpp:101-162): the rows the oracle's profile fields give, printed with
+    precision 10, are the reference's rows."""
+    o = oracle.OracleCase(N, N, tipo, chi, xi, tau=0.7, beta=0.8, A=A).init_strip(p, q)
+    r = oracle.RefStrip(N, tipo, p, q, chi, xi, tau=0.7, beta=0.8, A=A)
+    o.step(80)
+    r.step(80)
+    r.write_perfil(tmp_path)
+    f = o.fields(1)
+    m = math.sqrt(p * p + q * q)
+    rows = []
+    for y in range(N):
+        for x in range(N):
+            k = x + y * N
+            rho = f["rho_R"][k] + f["rho_B"][k]
+            s = (p * x + q * y) % N
+            d = s - 0.5 * N
+            if d >= 0.5 * N:
+                d -= N
+            if d < -0.5 * N:
+                d += N
+            d = -d / m
+            if rho > 0 and abs(d) < 12.0:
+                rows.append(" ".join("%.10g" % v for v in (d, f["rho_R"][k] / rho, rho, f["ux"][k], f["uy"][k])))
+    got = (tmp_path / "perfil.dat").read_text().splitlines()
+    assert got[0] == "# d  c=rho_R/rho  rho  ux  uy"
+    assert got[1:] == rows

@@ -6,6 +6,7 @@ restated here; where the reference's own analisar_lote.py is at hand it is also 
 folders of its batches and compared."""
 import csv
 import importlib.util
+import os
 import math
 import subprocess
 from pathlib import Path
@@ -14,7 +15,8 @@ import pytest
 
 REPO = Path(__file__).resolve().parent.parent
 BIN = REPO / "interfacial-tension-operators-lbm_b200" / "bin" / "itlbm_summary"
-REF = Path("/root/reference")
+# the reference project, where it is at hand ($ITLBM_REFERENCE): its own analisar_lote.py is then run too
+REF = Path(os.environ.get("ITLBM_REFERENCE", "")) if os.environ.get("ITLBM_REFERENCE") else None
 
 COLS = ['operador', 'chi', 'xi', 'tau', 'beta', 'fat_R_B', 'v0', 'nx', 'R_ini', 'sigma_nominal', 'estado',
         'passo_falha', 'passos', 'sigma_med', 'umax_med', 'urms_med', 'umax_sigma', 'Ca_s', 'a4_med', 'a8_med',
@@ -125,7 +127,8 @@ def test_strip_rows_and_missing_folder(tmp_path):
     assert len(read_csv(out)) == 2
 
 
-@pytest.mark.skipif(not (REF / "analisar_lote.py").exists(), reason="the reference is not at hand")
+@pytest.mark.skipif(REF is None or not (REF / "analisar_lote.py").exists(),
+                    reason="the reference is not at hand (set ITLBM_REFERENCE)")
 def test_reference_tables_on_stored_folders(tmp_path):
     spec = importlib.util.spec_from_file_location("analisar_lote", REF / "analisar_lote.py")
     al = importlib.util.module_from_spec(spec)
@@ -140,3 +143,25 @@ def test_reference_tables_on_stored_folders(tmp_path):
     for e, g in zip(ref_rows, got):
         for k, v in e.items():
             assert same(v, g[k]), (e["pasta"], k, v, g[k])
+
+
+def test_stored_folders_match_analisar_lote_rows(tmp_path, golden):
+    """Three stored Lotes/E2 folders (tests/golden/analisar_e2.json) and the rows the reference's own
+    analisar_lote.coleta made of them: itlbm_summary writes the same rows."""
+    import json
+    fixture = json.loads((REPO / "tests" / "golden" / "analisar_e2.json").read_text())
+    assert len(fixture) == 3
+    root = tmp_path / "E2"
+    dirs = []
+    for f in fixture:
+        d = root / f["pasta"]
+        d.mkdir(parents=True)
+        (d / "resumo.dat").write_text(f["resumo.dat"])
+        (d / "laplace.dat").write_text(f["laplace.dat"])
+        dirs.append(d)
+    out = tmp_path / "e2.csv"
+    assert run(out, root, *dirs).returncode == 0
+    got = read_csv(out)
+    for f, g in zip(fixture, got):
+        for k, v in f["row"].items():
+            assert same(float("nan") if v is None else v, g[k]), (f["pasta"], k, v, g[k])

@@ -172,7 +172,10 @@ int  itlbm_case_diag_drop(itlbm_case *c, int step, double x_ini, double y_ini, i
  *     ITLBM_STATIC_DIAG_MAX_NODES nodes and sides of at most ITLBM_STATIC_DIAG_MAX_SIDE; larger
  *     cases get ITLBM_E_ARG (use itlbm_case_diag_drop).
  *   - The first call on a device looks the array's address up (cudaGetSymbolAddress, with that
- *     device current); make it before any stream capture begins.
+ *     device current); make it before any stream capture begins.  Under CUDA's lazy module loading
+ *     (the default since CUDA 12.2) that first call is also when the device commits the array's
+ *     14 MiB, so make it while the device still has that much free, before a case pool takes the
+ *     rest of its memory.
  *   - Nothing has to start at zero: every call clears what it accumulates into.
  *   - Calls that overlap in time on the same device (from several host threads) share the scratch
  *     and race; serialize them.  A call returns only after its stream is synchronized. */
@@ -241,8 +244,10 @@ typedef struct itlbm_batch_config {
     int    diag_every;        /* diagnostic interval; 0 = 500                                     */
     int    ctas_per_sm;       /* launch shape of the step kernels: < 0 = one CTA per tile of the   */
                               /* work table; > 0 = that many persistent CTAs per SM striding over */
-                              /* it; 0 = autotune: the first full replay times the two (persistent */
-                              /* at the occupancy limit) and keeps the faster (same results)       */
+                              /* it; 0 = autotune: the first full replay times the tilings (narrow */
+                              /* edge tiles or 32 x 8 throughout) and the two launch shapes        */
+                              /* (persistent at the occupancy limit) and keeps the faster of each  */
+                              /* (same results)                                                     */
 } itlbm_batch_config;
 
 enum { ITLBM_EV_DIAG = 0, ITLBM_EV_DONE = 1, ITLBM_EV_UNSTABLE = 2 };
@@ -271,6 +276,9 @@ typedef struct itlbm_batch_stats {
     int       launch_mode;    /* launch shape in use: -1 one CTA per tile, 0 persistent CTAs at   */
                               /* the occupancy limit, k > 0 k persistent CTAs per SM               */
     int       held;           /* finished cases kept for itlbm_batch_read_fields (not in `active`) */
+    int       narrow_edges;   /* tiling in use: 1 the partial last tile column of a case in 16 x 16 */
+                              /* or 8 x 32 tiles, 0 32 x 8 tiles throughout (autotuned like the    */
+                              /* launch shape; the results do not depend on it)                     */
 } itlbm_batch_stats;
 
 /* No case memory is allocated until cases are admitted. */

@@ -113,7 +113,7 @@ class BatchStats(C.Structure):
                 ("node_updates", C.c_longlong), ("device_ms", C.c_double), ("hbm_used", C.c_size_t),
                 ("replays", C.c_int), ("captures", C.c_int), ("diag_ms", C.c_double),
                 ("advance_ms", C.c_double), ("admit_ms", C.c_double), ("capture_ms", C.c_double),
-                ("launch_mode", C.c_int), ("held", C.c_int)]
+                ("launch_mode", C.c_int), ("held", C.c_int), ("narrow_edges", C.c_int)]
 
 
 class ItlbmError(RuntimeError):

@@ -62,11 +62,18 @@ void fill_params(CaseDev &c, const itlbm_operador &op, double tau, double A_fact
 
 cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
                         const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
-                        cudaStream_t s) {
-    if (prec == ITLBM_PREC_F64) return launch_step_f64(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
-    if (prec == ITLBM_PREC_F32_FOLD) return launch_step_fold(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
+                        int shape, cudaStream_t s) {
+    if (prec == ITLBM_PREC_F64)
+        return launch_step_f64(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
+    if (prec == ITLBM_PREC_F32_FOLD)
+        return launch_step_fold(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
     return march ? launch_march_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s)
-                 : launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s);
+                 : launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
+}
+
+bool narrow_edges_default() {
+    const char *v = getenv("ITLBM_NARROW_EDGES");
+    return !(v && std::strcmp(v, "0") == 0);
 }
 
 bool march_default() {
@@ -87,10 +94,20 @@ void case_layout(CaseDev &h, int nx, int ny, int prec, bool march) {
     h.m_items = h.m_strips * ((ny + MARCH_SEG - 1) / MARCH_SEG);
 }
 
-int case_items(const CaseDev &h) { return h.march ? h.m_items : h.tiles; }
-
-int item_code(const CaseDev &h, int k) {
-    return h.march ? k : (int)(((unsigned)(k / h.tiles_x) << 16) | (unsigned)(k % h.tiles_x));
+void case_tiles(const CaseDev &h, bool narrow_edges, int case_id, std::vector<TileRef> *out) {
+    if (h.march) {
+        for (int k = 0; k < h.m_items; k++) out[SHAPE_32x8].push_back(TileRef{case_id, k});
+        return;
+    }
+    const int r = h.nx % TX;                               // columns of a partial last tile column
+    const int edge = !narrow_edges || r == 0 ? SHAPE_32x8 : (r <= 8 ? SHAPE_8x32 : (r <= 16 ? SHAPE_16x16 : SHAPE_32x8));
+    const int full = edge == SHAPE_32x8 ? h.tiles_x : h.tiles_x - 1;  // columns of 32 x 8 tiles
+    for (int ty = 0; ty < (h.ny + TY - 1) / TY; ty++)
+        for (int tx = 0; tx < full; tx++) out[SHAPE_32x8].push_back(TileRef{case_id, tile_code(tx * TX, ty * TY)});
+    if (edge != SHAPE_32x8) {
+        const int eh = shape_h(edge);
+        for (int y0 = 0; y0 < h.ny; y0 += eh) out[edge].push_back(TileRef{case_id, tile_code(full * TX, y0)});
+    }
 }
 
 cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf) {
@@ -116,8 +133,9 @@ struct itlbm_case {
     itlbm_case_desc desc{};
     CaseDev host{};
     CaseDev *dev = nullptr;
-    TileRef *tiles = nullptr;
+    TileRef *tiles = nullptr;       // the case's tiles grouped by shape: [tile_off[s], tile_off[s + 1])
     int ntiles = 0;
+    int tile_off[NSHAPE + 1] = {};
     void *mem = nullptr;
     double *aux = nullptr;
     double *tmp = nullptr;  // export / import staging (2 * 19 * n doubles)
@@ -251,9 +269,13 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
         return cuda_fail(e, "state tensor map");
     }
     h.aux = nullptr;
-    c->ntiles = case_items(h);
-    std::vector<TileRef> tl(c->ntiles);
-    for (int t = 0; t < c->ntiles; t++) tl[t] = TileRef{0, item_code(h, t)};
+    std::vector<TileRef> by_shape[NSHAPE], tl;
+    case_tiles(h, narrow_edges_default(), 0, by_shape);
+    for (int sh = 0; sh < NSHAPE; sh++) {
+        c->tile_off[sh] = (int)tl.size();
+        tl.insert(tl.end(), by_shape[sh].begin(), by_shape[sh].end());
+    }
+    c->tile_off[NSHAPE] = c->ntiles = (int)tl.size();
     if ((e = cudaMalloc(&c->tiles, sizeof(TileRef) * c->ntiles)) != cudaSuccess ||
         (e = cudaMalloc(&c->dev, sizeof(CaseDev))) != cudaSuccess) {
         itlbm_case_destroy(c);
@@ -301,9 +323,13 @@ int itlbm_case_step(itlbm_case *c, int nsteps, int flags, void *stream) {
     for (int i = 0; i < nsteps; i++) {
         const int k = (int)(c->steps + i);
         const int aux_k = (keep && i == nsteps - 1) ? k : -1;
-        cudaError_t e = launch_step(c->dev, c->tiles, c->ntiles, nullptr, c->ntiles, k, aux_k,
-                                    c->host.prec, c->host.march != 0, s);
-        if (e != cudaSuccess) return cuda_fail(e, "step kernel");
+        for (int sh = 0; sh < NSHAPE; sh++) {  // the tile shapes of one step touch disjoint nodes
+            const int n = c->tile_off[sh + 1] - c->tile_off[sh];
+            if (n == 0) continue;
+            cudaError_t e = launch_step(c->dev, c->tiles + c->tile_off[sh], n, nullptr, n, k, aux_k,
+                                        c->host.prec, c->host.march != 0, sh, s);
+            if (e != cudaSuccess) return cuda_fail(e, "step kernel");
+        }
     }
     c->steps += nsteps;
     c->aux_valid = keep ? 1 : 0;

@@ -71,10 +71,16 @@ size_t case_bytes(const itlbm_case_desc &d, bool &need_aux) {
     return (size_t)2 * 2 * planes_of(d.precision) * stride * elem + (need_aux ? (size_t)4 * stride * 8 : 0);
 }
 
-// the work tables, one per storage form: [0] FP64, [1] FP32, [2] FP32 fold
-constexpr int NTAB = 3;
+// the work tables, per storage form: [0] FP64, [1] FP32, [2] FP32 fold
+// ... and one per tile shape within each: table p holds storage form p / NSHAPE, shape p % NSHAPE
+constexpr int NPREC = 3;
+constexpr int NTAB = NPREC * NSHAPE;
 int table_of(int prec) { return prec == ITLBM_PREC_F64 ? 0 : (prec == ITLBM_PREC_F32 ? 1 : 2); }
-int prec_of_table(int p) { return p == 0 ? ITLBM_PREC_F64 : (p == 1 ? ITLBM_PREC_F32 : ITLBM_PREC_F32_FOLD); }
+int prec_of_table(int p) {
+    p /= NSHAPE;
+    return p == 0 ? ITLBM_PREC_F64 : (p == 1 ? ITLBM_PREC_F32 : ITLBM_PREC_F32_FOLD);
+}
+int shape_of_table(int p) { return p % NSHAPE; }
 
 const double U_LIMITE = 0.4;  // Imm_OPS.cpp:45
 
@@ -103,7 +109,7 @@ struct itlbm_batch {
     std::vector<int> free_slots;
     std::vector<CaseDev> h_cases;
     CaseDev *d_cases = nullptr;
-    TileRef *d_tiles[NTAB] = {};  // per storage form (table_of)
+    TileRef *d_tiles[NTAB] = {};  // per storage form and tile shape
     int tiles_cap[NTAB] = {};
     int *d_ntiles = nullptr;
     bool tables_dirty = true;
@@ -114,6 +120,9 @@ struct itlbm_batch {
     // k persistent CTAs per SM; with ctas_per_sm = 0 the first full replay times -1 against 0
     int mode = -1;
     bool tuning = false;
+    // a partial last tile column of a case in narrow tiles (16 x 16, 8 x 32) instead of 32 x 8; with
+    // ctas_per_sm = 0 the first full replay times both tilings and keeps the faster
+    bool narrow = true;
     cudaEvent_t tev[2] = {};
     bool march = false;  // FP32 cases run the marching kernel
     cudaGraphExec_t graph = nullptr;
@@ -175,9 +184,7 @@ int upload_tables(itlbm_batch *b) {
     for (Active *a : b->slots) {
         if (!a || a->held) continue;
         const CaseDev &c = b->h_cases[a->slot];
-        const int p = table_of(a->desc.precision);
-        const int n = case_items(c);
-        for (int k = 0; k < n; k++) t[p].push_back(TileRef{a->slot, item_code(c, k)});
+        case_tiles(c, b->narrow, a->slot, &t[table_of(a->desc.precision) * NSHAPE]);
     }
     int n[NTAB];
     for (int p = 0; p < NTAB; p++) {
@@ -212,7 +219,8 @@ cudaError_t enqueue_steps(itlbm_batch *b, int k0, int k1) {
         for (int p = 0; p < NTAB; p++)
             for (int k = k0; k < k1 && b->grid[p] > 0 && e == cudaSuccess; k++)
                 e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
-                                prec_of_table(p), p == 1 && b->march, b->stream);
+                                prec_of_table(p), prec_of_table(p) == ITLBM_PREC_F32 && b->march,
+                                shape_of_table(p), b->stream);
         return e;
     }
     if ((e = cudaEventRecord(b->ev_fork, b->stream)) != cudaSuccess) return e;
@@ -221,7 +229,8 @@ cudaError_t enqueue_steps(itlbm_batch *b, int k0, int k1) {
         if ((e = cudaStreamWaitEvent(b->side[p], b->ev_fork, 0)) != cudaSuccess) return e;
         for (int k = k0; k < k1 && e == cudaSuccess; k++)
             e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
-                            prec_of_table(p), p == 1 && b->march, b->side[p]);
+                            prec_of_table(p), prec_of_table(p) == ITLBM_PREC_F32 && b->march,
+                            shape_of_table(p), b->side[p]);
         if (e != cudaSuccess) return e;
         if ((e = cudaEventRecord(b->ev_join[p], b->side[p])) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(b->stream, b->ev_join[p], 0)) != cudaSuccess) return e;
@@ -268,32 +277,50 @@ long long updates_in(const itlbm_batch *b, int k0, int k1) {
     return u;
 }
 
-// Autotuning of the launch shape on the first full replay: sub-steps [0, M) with one CTA per table
-// entry (M = K / 16), [M, 2M) with persistent CTAs at the occupancy limit, both timed with events; the faster
-// (per node update) runs the rest of the replay and is captured into the graph.  Both shapes run the
-// same kernel on the same tiles, so the results do not depend on the choice.
+// Autotuning on the first full replay, in timed windows of M = K / 16 sub-steps (CUDA events, rate
+// per node update): the tiling -- narrow tiles at the partial last tile column of a case against
+// 32 x 8 tiles throughout -- with one CTA per table entry, then persistent CTAs at the occupancy limit
+// with the better tiling.  The faster of each runs the rest of the replay and is captured into the
+// graph.  Every choice runs the same arithmetic on every node, so the results do not depend on it.
 int tune_and_run(itlbm_batch *b, int K) {
     const int M = std::max(2, K / 16);
-    const int modes[2] = {-1, 0};
-    double rate[2] = {0, 0};
-    cudaError_t e = cudaSuccess;
-    for (int c = 0; c < 2 && e == cudaSuccess; c++) {
-        b->mode = modes[c];
+    int k0 = 0;
+    auto window = [&](int mode, bool narrow, double &rate) -> int {
+        if (narrow != b->narrow) {
+            b->narrow = narrow;
+            const int r = upload_tables(b);
+            if (r) return r;
+        }
+        b->mode = mode;
         set_grids(b);
         cudaEventRecord(b->tev[0], b->stream);
-        e = enqueue_steps(b, c * M, (c + 1) * M);
+        cudaError_t e = enqueue_steps(b, k0, k0 + M);
         cudaEventRecord(b->tev[1], b->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(b->tev[1]);
         float ms = 0;
         if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->tev[0], b->tev[1]);
-        rate[c] = ms > 0 ? (double)updates_in(b, c * M, (c + 1) * M) / ms : 0.0;
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "launch-shape tuning");
+        if (e != cudaSuccess) return cuda_fail(e, "autotuning window");
+        rate = ms > 0 ? (double)updates_in(b, k0, k0 + M) / ms : 0.0;
+        k0 += M;
+        return ITLBM_OK;
+    };
+    double r_narrow = 0, r_uniform = 0, r_persist = 0;
+    int r;
+    if ((r = window(-1, true, r_narrow)) != ITLBM_OK || (r = window(-1, false, r_uniform)) != ITLBM_OK)
+        return r;
+    const bool narrow = r_narrow >= r_uniform;
+    if ((r = window(0, narrow, r_persist)) != ITLBM_OK) return r;
     // persistent CTAs only when clearly faster (the two are within noise on small tables)
-    b->mode = rate[1] > 1.02 * rate[0] ? 0 : -1;
+    const int mode = r_persist > 1.02 * std::max(r_narrow, r_uniform) ? 0 : -1;
+    if (b->narrow != narrow) {
+        b->narrow = narrow;
+        if ((r = upload_tables(b)) != ITLBM_OK) return r;
+    }
+    b->mode = mode;
     b->tuning = false;
     set_grids(b);
-    if ((e = enqueue_steps(b, 2 * M, K)) != cudaSuccess) return cuda_fail(e, "step launches");
+    cudaError_t e;
+    if ((e = enqueue_steps(b, k0, K)) != cudaSuccess) return cuda_fail(e, "step launches");
     return capture_graph(b);
 }
 
@@ -937,6 +964,7 @@ int itlbm_batch_stats_get(const itlbm_batch *b, itlbm_batch_stats *out) {
     out->active = 0;
     for (Active *a : b->slots) out->active += (a && !a->held) ? 1 : 0;
     out->held = b->nheld;
+    out->narrow_edges = b->narrow ? 1 : 0;
     out->pending = (int)b->pending.size();
     out->finished = b->finished;
     out->node_updates = b->node_updates;

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/itlbm.h"
 
@@ -14,22 +15,19 @@ namespace itlbm {
 
 constexpr int NV = 19;
 
-// Tile of the fused step: TX x TY interior nodes, one per thread; the phase field is staged with a
-// halo of up to HMAX nodes (1 for P1/P3/F3, 2 for F1/F2).
-#ifndef ITLBM_TILE_COLS
-#define ITLBM_TILE_COLS 32
-#endif
-constexpr int TX = ITLBM_TILE_COLS;
-#ifndef ITLBM_TILE_ROWS
-#define ITLBM_TILE_ROWS 8
-#endif
-constexpr int TY = ITLBM_TILE_ROWS;
+// Tiles of the fused step: 256 interior nodes, one per thread, in one of three shapes; the phase
+// field is staged with a halo of up to HMAX nodes (1 for P1/P3/F3, 2 for F1/F2).  A case is tiled by
+// 32 x 8 tiles (a warp per row of 32 nodes); the last tile column, when nx is not a multiple of 32,
+// can instead be cut into 16 x 16 or 8 x 32 tiles (a warp covering 2 or 4 row pieces of 16 or 8
+// nodes), which leaves fewer threads idle beyond the box's edge.  The shape changes no result: a
+// node's update is the same whichever tile computes it.
+constexpr int TX = 32;             // the base shape 32 x 8
+constexpr int TY = 8;
 constexpr int HMAX = 2;
-constexpr int PX = TX + 2 * HMAX;  // staged phase tile width
-constexpr int PY = TY + 2 * HMAX;  // staged phase tile height
-constexpr int QX = TX + 2;         // ring-1 region of the F1/F2 auxiliary fields
-constexpr int QY = TY + 2;
-constexpr int STEP_THREADS = TX * TY;
+constexpr int STEP_THREADS = 256;
+enum { SHAPE_32x8 = 0, SHAPE_16x16 = 1, SHAPE_8x32 = 2, NSHAPE = 3 };
+__host__ __device__ constexpr int shape_w(int s) { return s == SHAPE_32x8 ? 32 : (s == SHAPE_16x16 ? 16 : 8); }
+__host__ __device__ constexpr int shape_h(int s) { return STEP_THREADS / shape_w(s); }
 // Marching kernel of the FP32 step (itlbm_march.cu): work items are 32-column strips of MARCH_SEG rows.
 constexpr int MARCH_W = 32;
 constexpr int MARCH_SEG = 64;
@@ -122,25 +120,26 @@ struct CaseDev {
 };
 
 // An entry of the work table: case index and work item within that case.  For the tile kernel the
-// item is the tile's column and row packed as (ty << 16) | tx (no division in the kernel); for the
-// marching kernel it is the linear item index.
+// item is the tile's origin in units of 8 nodes, packed as ((y0 / 8) << 16) | (x0 / 8) (no division
+// in the kernel); for the marching kernel it is the linear item index.
 struct TileRef {
     int case_id;
     int tile;
 };
-// Boxes whose tile columns or rows would not fit 16 bits are refused at creation.
+// Boxes whose sides do not fit 16 bits in units of 8 nodes are refused at creation.
 constexpr int MAX_TILE_COORD = 65535;
 inline bool box_tileable(int nx, int ny) {
-    return (nx + TX - 1) / TX <= MAX_TILE_COORD && (ny + TY - 1) / TY <= MAX_TILE_COORD;
+    return (nx + 7) / 8 <= MAX_TILE_COORD && (ny + 7) / 8 <= MAX_TILE_COORD;
 }
+inline int tile_code(int x0, int y0) { return (int)(((unsigned)(y0 / 8) << 16) | (unsigned)(x0 / 8)); }
 
 // ---- kernel launchers (defined in the .cu files) -------------------------------------------
 cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
+                            const int *ntiles_dev, int grid, int k, int aux_k, int shape, cudaStream_t s);
 cudaError_t launch_step_f32(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
+                            const int *ntiles_dev, int grid, int k, int aux_k, int shape, cudaStream_t s);
 cudaError_t launch_step_fold(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s);
+                             const int *ntiles_dev, int grid, int k, int aux_k, int shape, cudaStream_t s);
 int step_occupancy_f64();
 int step_occupancy_f32();
 int step_occupancy(int prec);
@@ -157,15 +156,20 @@ size_t march_smem_bytes();
 // Layout of a case's state and its work items (tiles or marching items), and the binding of its
 // state block: pointers and, for the marching kernel, the tensor map.
 void case_layout(CaseDev &h, int nx, int ny, int prec, bool march);
-int case_items(const CaseDev &h);
-int item_code(const CaseDev &h, int k);  // the TileRef::tile of work item k
+// The work items of a case with index case_id, appended to out[shape] (NSHAPE vectors): the marching kernel's items
+// (all in out[SHAPE_32x8]), or its tiles -- 32 x 8, and with narrow_edges a last partial tile column
+// of r = nx mod 32 columns cut into 8 x 32 tiles (r <= 8) or 16 x 16 tiles (8 < r <= 16).
+void case_tiles(const CaseDev &h, bool narrow_edges, int case_id, std::vector<TileRef> *out);
 cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf);
 // The FP32 kernel the library uses: the tile kernel, or the marching kernel with ITLBM_STEP_KERNEL=march.
 bool march_default();
-// `march` selects the FP32 kernel; FP64 always runs the tile kernel.
+// Whether single cases cut a partial last tile column into narrow tiles (ITLBM_NARROW_EDGES=0: no).
+bool narrow_edges_default();
+// `march` selects the FP32 kernel; FP64 always runs the tile kernel; `shape` is the tile shape of
+// every entry of `tiles` (tile kernel only).
 cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
                         const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
-                        cudaStream_t s);
+                        int shape, cudaStream_t s);
 cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
                         cudaStream_t s);  // single cases: stages the profile, waits
 size_t profile_len(const CaseDev &c, const itlbm_case_desc &d);

@@ -10,7 +10,8 @@
 // `dst`, as propag_site does (SimBoltz_Functions/LBM_functions.cpp:1220-1247).  The post-collision
 // values the diagnostics need are therefore dst(x + c_i, i).
 //
-// One CTA handles a TX x TY tile of one case (the work table says which).  It stages rho^N for the
+// One CTA handles a tile of 256 nodes of one case (the work table says which; its shape -- 32 x 8, or
+// 16 x 16 / 8 x 32 at the edge of a box whose width is not a multiple of 32 -- is that of the kernel).  It stages rho^N for the
 // tile plus a halo of 1 (P1, P3, F3) or 2 (F1, F2) nodes in shared memory -- the halo nodes are
 // re-read from L2, where the neighbouring tiles keep them -- then evaluates the mediator gradient,
 // the force of class F on a ring-1 region of auxiliary fields, and collides.  No mediator
@@ -88,10 +89,13 @@ __device__ __forceinline__ int wrap_near(int a, int n) {
 // lanes on each bank).
 constexpr int AUXS = 7;
 
-template <class S>
+// Shared memory of a W x Hh tile.
+template <class S, int W, int Hh>
 struct SmemT {
+    static constexpr int PX = W + 2 * HMAX, PY = Hh + 2 * HMAX;  // staged phase tile
+    static constexpr int QX = W + 2, QY = Hh + 2;                // ring-1 region of the F1/F2 auxiliaries
     S phi[PY][PX];        // rho^N of tile + halo (HMAX), position (px, py) = global (x0-2+px, y0-2+py)
-    S rsum[2][PY * PX - TX * TY];  // halo ring: the two colour sums of each ring node
+    S rsum[2][PY * PX - W * Hh];  // halo ring: the two colour sums of each ring node
     S g[QY][QX][3];       // ring-1 gradient (F1, F2)
     S aux[QY][QX][AUXS];  // ring-1 normal (F1) or stress (F2), 6 values at an odd stride
 };
@@ -105,28 +109,29 @@ __device__ __forceinline__ float phase_of(float drho, float D, const CaseDev &c)
     return D / ((float)c.rho0 + drho);
 }
 
-// ring position r -> staged-tile coordinates (px, py) for a halo of H (1 or 2) around the TX x TY
+// ring position r -> staged-tile coordinates (px, py) for a halo of H (1 or 2) around the W x Hh
 // interior; consecutive r run along x in the top and bottom bands, so loads of consecutive r
-// coalesce.  The divisions by the band width W are a multiply by ceil(2^16 / W) and a shift, exact
-// for r < 2^16 / W (r stays below 2 x 176 here).
+// coalesce.  The divisions by the band width B are a multiply by ceil(2^16 / B) and a shift, exact
+// for r < 2^16 / B (r stays below the band length, at most 2 x 36, here).
+template <int W, int Hh>
 __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
-    constexpr int W1 = TX + 2, W2 = TX + 4;
+    constexpr int W1 = W + 2, W2 = W + 4;
     constexpr int M1 = (65536 + W1 - 1) / W1, M2 = (65536 + W2 - 1) / W2;
-    static_assert(2 * ((TX + 4) * (TY + 4) - TX * TY) * M1 < (1 << 30), "ring index range");
-    const int W = TX + 2 * H, M = H == 1 ? M1 : M2;
-    const int nTop = H * W;
+    static_assert(2 * W2 < 65536 / W2, "ring index range: the multiply-shift division is exact");
+    const int B = W + 2 * H, M = H == 1 ? M1 : M2;
+    const int nTop = H * B;
     if (r < 2 * nTop) {
         const int band = r < nTop ? 0 : 1;
         r -= band * nTop;
         const int q = (r * M) >> 16;
-        py = band ? HMAX + TY + q : HMAX - H + q;
-        px = HMAX - H + (r - q * W);
+        py = band ? HMAX + Hh + q : HMAX - H + q;
+        px = HMAX - H + (r - q * B);
     } else {
         r -= 2 * nTop;
         const int q = H == 1 ? (r >> 1) : (r >> 2);  // r / (2 H)
         const int k = r - q * 2 * H;
         py = HMAX + q;
-        px = k < H ? HMAX - H + k : HMAX + TX + (k - H);
+        px = k < H ? HMAX - H + k : HMAX + W + (k - H);
     }
 }
 
@@ -139,19 +144,20 @@ __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
 //   phase B  F1 / F2: gradient and normal or stress on the ring-1 region;
 //   phase C  mediator gradient, force, collision, recolouring, push to x + c_i.
 // FOLD (FP32 only): the nine in-plane classes per colour instead of the 19 populations.
-template <class S, bool FOLD = false>
+template <class S, bool FOLD, int W, int Hh>
 __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int aux_k,
-                                          SmemT<S> &sm) {
+                                          SmemT<S, W, Hh> &sm) {
     constexpr int NP = FOLD ? NK : NV;  // storage planes per colour
+    constexpr int QX = SmemT<S, W, Hh>::QX, QY = SmemT<S, W, Hh>::QY;
     const int tid = threadIdx.x;
-    const int lx = tid % TX, ly = tid / TX;
+    const int lx = tid % W, ly = tid / W;
     const int nx = c.nx, ny = c.ny, pitch = c.pitch;
     const long long stride = c.stride;
     // plane q of a buffer (uniform across the CTA); offsets within a plane are 32-bit (a plane holds
     // fewer than 2^31 elements: boxes are capped at 2^30 nodes and 65535 tile rows)
     auto plane = [stride](auto *buf, int q) { return buf + (long long)q * stride; };
-    const int x0 = (int)((unsigned)tile & 0xFFFFu) * TX, y0 = (int)((unsigned)tile >> 16) * TY;
-    const int xe = min(x0 + TX, nx), ye = min(y0 + TY, ny);  // end of the valid interior
+    const int x0 = (int)((unsigned)tile & 0xFFFFu) * 8, y0 = (int)((unsigned)tile >> 16) * 8;
+    const int xe = min(x0 + W, nx), ye = min(y0 + Hh, ny);  // end of the valid interior
     const int H = c.halo;
     const int cur = (c.parity0 + k) & 1;
     const S *__restrict__ src = (const S *)c.buf[cur];
@@ -190,11 +196,11 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         }
         sm.phi[ly + HMAX][lx + HMAX] = phase_of(sa, sb, c);
     }
-    const int nring = (TX + 2 * H) * (TY + 2 * H) - TX * TY;
+    const int nring = (W + 2 * H) * (Hh + 2 * H) - W * Hh;
     for (int it = tid; it < 2 * nring; it += STEP_THREADS) {
         const int colour = it >= nring ? 1 : 0, r = it - colour * nring;
         int px, py;
-        ring_pos(r, H, px, py);
+        ring_pos<W, Hh>(r, H, px, py);
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
         if (gx < xe + H && gy < ye + H) {
             const int off = wrap_near(gy, ny) * pitch + wrap_near(gx, nx);
@@ -210,7 +216,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     __syncthreads();
     for (int r = tid; r < nring; r += STEP_THREADS) {
         int px, py;
-        ring_pos(r, H, px, py);
+        ring_pos<W, Hh>(r, H, px, py);
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
         if (gx < xe + H && gy < ye + H) sm.phi[py][px] = phase_of(sm.rsum[0][r], sm.rsum[1][r], c);
     }
@@ -400,19 +406,33 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #define ITLBM_STEP_MIN_BLOCKS (ITLBM_F32_BLOCKS * 256 / STEP_THREADS)
 #endif
 
-template <class S, bool FOLD = false>
+template <class S, bool FOLD, int W>
 __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(const CaseDev *__restrict__ cases,
                                                        const TileRef *__restrict__ tiles,
                                                        int ntiles, const int *__restrict__ ntiles_dev,
                                                        int k, int aux_k) {
-    __shared__ SmemT<S> sm;
+    constexpr int Hh = STEP_THREADS / W;
+    __shared__ SmemT<S, W, Hh> sm;
     const int nt = ntiles_dev ? *ntiles_dev : ntiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const TileRef tr = tiles[t];
         const CaseDev &c = cases[tr.case_id];
         if (k >= c.chunk_len) continue;
-        step_tile<S, FOLD>(c, tr.tile, k, aux_k, sm);
+        step_tile<S, FOLD, W, Hh>(c, tr.tile, k, aux_k, sm);
     }
+}
+
+template <class S, bool FOLD>
+cudaError_t launch_shape(const CaseDev *cases_dev, const TileRef *tiles, int ntiles, const int *ntiles_dev,
+                         int grid, int k, int aux_k, int shape, cudaStream_t s) {
+    if (grid <= 0) return cudaSuccess;
+    switch (shape) {
+        case SHAPE_32x8: k_step<S, FOLD, 32><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k); break;
+        case SHAPE_16x16: k_step<S, FOLD, 16><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k); break;
+        case SHAPE_8x32: k_step<S, FOLD, 8><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -421,33 +441,27 @@ __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(co
 // rounds exactly as the reference's own code compiled with strict IEEE semantics) and without it.
 #ifdef ITLBM_STEP_F64
 cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s) {
-    if (grid <= 0) return cudaSuccess;
-    k_step<double><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
-    return cudaGetLastError();
+                            const int *ntiles_dev, int grid, int k, int aux_k, int shape, cudaStream_t s) {
+    return launch_shape<double, false>(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
 }
 int step_occupancy_f64() {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<double>, STEP_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<double, false, 32>, STEP_THREADS, 0);
     return n;
 }
 #else
 cudaError_t launch_step_f32(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                            const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s) {
-    if (grid <= 0) return cudaSuccess;
-    k_step<float><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
-    return cudaGetLastError();
+                            const int *ntiles_dev, int grid, int k, int aux_k, int shape, cudaStream_t s) {
+    return launch_shape<float, false>(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
 }
 int step_occupancy_f32() {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<float>, STEP_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<float, false, 32>, STEP_THREADS, 0);
     return n;
 }
 cudaError_t launch_step_fold(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                             const int *ntiles_dev, int grid, int k, int aux_k, cudaStream_t s) {
-    if (grid <= 0) return cudaSuccess;
-    k_step<float, true><<<grid, STEP_THREADS, 0, s>>>(cases_dev, tiles, ntiles, ntiles_dev, k, aux_k);
-    return cudaGetLastError();
+                             const int *ntiles_dev, int grid, int k, int aux_k, int shape, cudaStream_t s) {
+    return launch_shape<float, true>(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
 }
 #endif
 

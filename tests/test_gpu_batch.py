@@ -210,3 +210,27 @@ def test_held_cases_give_their_final_fields(gpu):
             assert np.array_equal(fa[key], fb[key]), (k, key)
         for key in ("rho_R", "rho_B", "ux", "uy"):
             assert np.array_equal(pa[key], pb[key]), (k, key)
+
+
+def test_tilings_agree_and_are_reported(gpu):
+    """The batch's autotuner times narrow edge tiles against 32 x 8 tiles throughout on its first full
+    replay (the windows switch tilings in the middle of it) and reports its choice; no bit changes:
+    every diagnostic equals that of the same case run alone."""
+    cases = [(45, 3, 0.225, 1, 0, (1, 0)), (58, 12, 0.1, 1, 0, (1, 0)), (40, 11, 0.1, 2, 1, (2, 1)),
+             (71, 13, 0.1, 0, 0, (1, 0)), (33, 1, 0.225, 1, 0, (1, 0)), (48, 12, 0.1, 2, 0, (1, 0))]
+    descs = [mkdesc(gpu, nx, t, A=A, prec=pr, geometry=g, p=pq[0], q=pq[1]) for nx, t, A, pr, g, pq in cases]
+    alone = [run_alone(gpu, d, 300)[0] for d in descs]
+    with gpu.Batch(chunk=160) as b:
+        for k, d in enumerate(descs):
+            b.submit(d, 300, k)
+        events = []
+        for _ in range(20):
+            b.advance()
+            events += b.poll()
+            st = b.stats()
+            if st.active == 0 and st.pending == 0:
+                break
+        assert st.narrow_edges in (0, 1) and st.launch_mode in (-1, 0)
+    for k, c in enumerate(cases):
+        rows = [(e.drop if c[4] == 0 else e.strip).as_dict() for e in events if e.tag == k and e.kind == gpu.EV_DIAG]
+        assert rows == alone[k], k

@@ -358,3 +358,25 @@ def test_fields_need_the_force_of_class_f(gpu):
     c.step(1, keep_aux=True)
     assert np.isfinite(c.read_profile()["ux"]).all()
     c.close()
+
+
+# ---- tile shapes --------------------------------------------------------------------------------
+@pytest.mark.parametrize("prec", [0, 1, 2], ids=["fp64", "fp32", "fold"])
+@pytest.mark.parametrize("nx", [7, 40, 45, 61, 64, 100])
+def test_tile_shapes_agree(gpu, monkeypatch, prec, nx):
+    """A partial last tile column cut into 8 x 32 (nx mod 32 <= 8) or 16 x 16 tiles (<= 16) gives the
+    same bits as 32 x 8 tiles throughout, for every storage form and both halo widths."""
+    out = {}
+    for narrow in ("1", "0"):
+        monkeypatch.setenv("ITLBM_NARROW_EDGES", narrow)
+        res = []
+        for tipo, A in ((3, 0.225), (12, 0.1), (11, 0.1)):
+            c = gpu_case(gpu, nx, 52, tipo, 0.5, 1.569988, A, tau=0.8, radius=nx / 5 + 2, v0=0.05, prec=prec)
+            c.step(37, keep_aux=True)
+            res.append((c.read_pops(0), c.read_fields()))
+            c.close()
+        out[narrow] = res
+    for (pa, fa), (pb, fb) in zip(out["1"], out["0"]):
+        assert same(pa, pb)
+        for k in fa:
+            assert np.array_equal(fa[k], fb[k]), k

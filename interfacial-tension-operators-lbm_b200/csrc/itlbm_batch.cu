@@ -129,8 +129,8 @@ struct itlbm_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // one chain of step launches per non-empty table, each on its own stream between a fork and a
     // join on `stream`: the tables hold different cases, so their steps need no order between them
-    cudaStream_t side[NTAB] = {};
-    cudaEvent_t ev_fork = nullptr, ev_join[NTAB] = {};
+    cudaStream_t side[NPREC] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[NPREC] = {};
     // diagnostics: the cases that fall due in an advance are measured together, drops and strips each
     // by one sequence of launches over a table of jobs, their scratch in per-case segments of one
     // block (grown on demand, up to DIAG_SCRATCH_LIMIT or the largest single case; more due cases than
@@ -209,31 +209,44 @@ int upload_tables(itlbm_batch *b) {
     return cudaStreamSynchronize(b->stream) == cudaSuccess ? ITLBM_OK : cuda_fail(cudaGetLastError(), "sync");
 }
 
-// Sub-steps [k0, k1) of every table on the batch stream: one table runs in line, several run as
-// parallel chains (fork, one chain per table on its own stream, join), in a capture or directly.
+// Sub-steps [k0, k1) of the tables of storage form pi on stream st.  The tables of one storage form
+// (one per tile shape) hold tiles of the same cases, so every sub-step launches them in turn on the
+// one stream: sub-step k of every tile of a case ends before any tile of it starts sub-step k + 1.
+cudaError_t enqueue_chain(itlbm_batch *b, int pi, int k0, int k1, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    for (int k = k0; k < k1 && e == cudaSuccess; k++)
+        for (int sh = 0; sh < NSHAPE && e == cudaSuccess; sh++) {
+            const int p = pi * NSHAPE + sh;
+            if (b->grid[p] > 0)
+                e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
+                                prec_of_table(p) == ITLBM_PREC_F32 && b->march, sh, st);
+        }
+    return e;
+}
+
+// Sub-steps [k0, k1) of every table on the batch stream: the storage forms hold different cases, so
+// one form runs in line and several run as parallel chains (fork, one chain per form on its own
+// stream, join), in a capture or directly.
 cudaError_t enqueue_steps(itlbm_batch *b, int k0, int k1) {
+    bool busy[NPREC] = {};
     int used = 0;
-    for (int p = 0; p < NTAB; p++) used += b->grid[p] > 0;
+    for (int pi = 0; pi < NPREC; pi++) {
+        for (int sh = 0; sh < NSHAPE; sh++) busy[pi] = busy[pi] || b->grid[pi * NSHAPE + sh] > 0;
+        used += busy[pi];
+    }
     cudaError_t e = cudaSuccess;
     if (used <= 1) {
-        for (int p = 0; p < NTAB; p++)
-            for (int k = k0; k < k1 && b->grid[p] > 0 && e == cudaSuccess; k++)
-                e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
-                                prec_of_table(p), prec_of_table(p) == ITLBM_PREC_F32 && b->march,
-                                shape_of_table(p), b->stream);
+        for (int pi = 0; pi < NPREC && e == cudaSuccess; pi++)
+            if (busy[pi]) e = enqueue_chain(b, pi, k0, k1, b->stream);
         return e;
     }
     if ((e = cudaEventRecord(b->ev_fork, b->stream)) != cudaSuccess) return e;
-    for (int p = 0; p < NTAB; p++) {
-        if (b->grid[p] <= 0) continue;
-        if ((e = cudaStreamWaitEvent(b->side[p], b->ev_fork, 0)) != cudaSuccess) return e;
-        for (int k = k0; k < k1 && e == cudaSuccess; k++)
-            e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1,
-                            prec_of_table(p), prec_of_table(p) == ITLBM_PREC_F32 && b->march,
-                            shape_of_table(p), b->side[p]);
-        if (e != cudaSuccess) return e;
-        if ((e = cudaEventRecord(b->ev_join[p], b->side[p])) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(b->stream, b->ev_join[p], 0)) != cudaSuccess) return e;
+    for (int pi = 0; pi < NPREC; pi++) {
+        if (!busy[pi]) continue;
+        if ((e = cudaStreamWaitEvent(b->side[pi], b->ev_fork, 0)) != cudaSuccess) return e;
+        if ((e = enqueue_chain(b, pi, k0, k1, b->side[pi])) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(b->ev_join[pi], b->side[pi])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(b->stream, b->ev_join[pi], 0)) != cudaSuccess) return e;
     }
     return e;
 }
@@ -672,7 +685,7 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
         itlbm_batch_destroy(b);
         return cuda_fail(e, "batch events");
     }
-    for (int p = 0; p < NTAB; p++)
+    for (int p = 0; p < NPREC; p++)
         if ((e = cudaStreamCreateWithFlags(&b->side[p], cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&b->ev_join[p], cudaEventDisableTiming)) != cudaSuccess) {
             itlbm_batch_destroy(b);
@@ -719,7 +732,7 @@ void itlbm_batch_destroy(itlbm_batch *b) {
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     for (int t = 0; t < 2; t++)
         if (b->tev[t]) cudaEventDestroy(b->tev[t]);
-    for (int p = 0; p < NTAB; p++) {
+    for (int p = 0; p < NPREC; p++) {
         if (b->ev_join[p]) cudaEventDestroy(b->ev_join[p]);
         if (b->side[p]) cudaStreamDestroy(b->side[p]);
     }

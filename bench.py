@@ -141,8 +141,9 @@ def batch_run(pkg, steps, warmup, world, sample_clocks, local, n_cases=600, prec
     upd = st1.node_updates - st0.node_updates
     assert upd % steps == 0 and st1.active == st0.active
     b.close()
-    global LAST_LAUNCH_MODE
+    global LAST_LAUNCH_MODE, LAST_TILING
     LAST_LAUNCH_MODE = st1.launch_mode
+    LAST_TILING = st1.narrow_edges
     return upd // steps, ms, (sampler.summary() if sampler else None), st1.active
 
 
@@ -596,6 +597,7 @@ REF_EVERY = 10  # the reference arm steps every 10th case of the batch mix (60 c
 
 
 LAST_LAUNCH_MODE = None  # launch shape the batch engine's autotuner chose in the last batch_run
+LAST_TILING = None  # and its tiling: 1 narrow tiles at a box's partial last column, 0 32 x 8 throughout
 
 
 def batch_config(nodes, ncases, world):
@@ -712,6 +714,8 @@ def main():
         launches = args.steps  # one FP32 launch per step; the FP64 table is empty, so nothing is launched for it
         cfg = batch_config(nodes, ncases, world)
         cfg["launch_shape"] = {-1: "one CTA per tile (autotuned)", 0: "persistent CTAs (autotuned)"}.get(mode, mode)
+        cfg["tiling"] = {1: "narrow tiles at partial last columns (autotuned)",
+                         0: "32x8 tiles throughout (autotuned)"}.get(LAST_TILING, LAST_TILING)
     else:
         nodes, ms, clocks = device_run(pkg, single, pkg.PREC_F32, args.steps, args.warmup, world,
                                        rank == 0, local)

@@ -24,6 +24,9 @@ int fail(int code, const std::string &msg) {
 }
 int cuda_fail(cudaError_t e, const char *what) {
     g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    // consume the runtime's record of the failure, so that a later call's cudaGetLastError does not
+    // report it again (a failed allocation leaves it set; a sticky error stays whatever is done)
+    cudaGetLastError();
     if (e == cudaErrorMemoryAllocation) return ITLBM_E_OOM;
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ITLBM_E_NODEVICE;
     return ITLBM_E_CUDA;
@@ -57,31 +60,41 @@ void fill_params(CaseDev &c, const itlbm_operador &op, double tau, double A_fact
     }
     c.kf = 0.75 * A_fact * op.xi;           // Operadores_tensao.cpp:240
     c.bf = 3.0 * A_fact / (8.0 * op.xi);    // Operadores_tensao.cpp:241
+    fill_shift(c, rho0, 0.0);
+}
+
+// The FP32 storage shift of a case (see CaseDev): the equilibrium at rho0 and U0 = (u0x, 0).
+void fill_shift(CaseDev &c, double rho0, double u0x) {
     c.rho0 = rho0;
+    c.u0x = u0x;
+    const double u2 = u0x * u0x;
+    c.j0x = (float)(rho0 * u0x);
+    c.u0b = (float)(rho0 * u2);
+    c.s0 = (float)(rho0 * (1.0 - 1.5 * u2));
+    c.sx = (float)(rho0 * (1.0 + 3.0 * u2));  // s0 + 4.5 rho0 u0x^2
+    c.j3 = (float)(3.0 * rho0 * u0x);
+    // the float operations of shift_of (itlbm_site.cuh), so that host and device agree to the bit
+    auto shift = [&](float w, int ex) { return w * (ex == 0 ? c.s0 : (ex > 0 ? c.sx + c.j3 : c.sx - c.j3)); };
+    for (int i = 0; i < NV; i++) c.sh[i] = shift(wgt<float>(i), cx(i));
+    for (int K = 0; K < NK; K++) c.shk[K] = shift(wk<float>(K), kx(K));
 }
 
 cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                        const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
+                        const int *ntiles_dev, int grid, int k, int aux_k, int prec,
                         int shape, cudaStream_t s) {
     if (prec == ITLBM_PREC_F64)
         return launch_step_f64(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
     if (prec == ITLBM_PREC_F32_FOLD)
         return launch_step_fold(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
-    return march ? launch_march_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, s)
-                 : launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
+    return launch_step_f32(cases_dev, tiles, ntiles, ntiles_dev, grid, k, aux_k, shape, s);
 }
 
 bool narrow_edges_default() {
     const char *v = getenv("ITLBM_NARROW_EDGES");
-    return !(v && std::strcmp(v, "0") == 0);
+    return v && std::strcmp(v, "1") == 0;
 }
 
-bool march_default() {
-    const char *v = getenv("ITLBM_STEP_KERNEL");
-    return v && std::strcmp(v, "march") == 0;
-}
-
-void case_layout(CaseDev &h, int nx, int ny, int prec, bool march) {
+void case_layout(CaseDev &h, int nx, int ny, int prec) {
     h.nx = nx;
     h.ny = ny;
     h.pitch = (nx + 31) / 32 * 32;
@@ -89,16 +102,9 @@ void case_layout(CaseDev &h, int nx, int ny, int prec, bool march) {
     h.tiles_x = (nx + TX - 1) / TX;
     h.tiles = h.tiles_x * ((ny + TY - 1) / TY);
     h.prec = prec;
-    h.march = (prec == ITLBM_PREC_F32 && march) ? 1 : 0;
-    h.m_strips = (nx + MARCH_W - 1) / MARCH_W;
-    h.m_items = h.m_strips * ((ny + MARCH_SEG - 1) / MARCH_SEG);
 }
 
 void case_tiles(const CaseDev &h, bool narrow_edges, int case_id, std::vector<TileRef> *out) {
-    if (h.march) {
-        for (int k = 0; k < h.m_items; k++) out[SHAPE_32x8].push_back(TileRef{case_id, k});
-        return;
-    }
     const int r = h.nx % TX;                               // columns of a partial last tile column
     const int edge = !narrow_edges || r == 0 ? SHAPE_32x8 : (r <= 8 ? SHAPE_8x32 : (r <= 16 ? SHAPE_16x16 : SHAPE_32x8));
     const int full = edge == SHAPE_32x8 ? h.tiles_x : h.tiles_x - 1;  // columns of 32 x 8 tiles
@@ -113,7 +119,8 @@ void case_tiles(const CaseDev &h, bool narrow_edges, int case_id, std::vector<Ti
 cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf) {
     h.buf[0] = mem;
     h.buf[1] = (char *)mem + per_buf;
-    return h.march ? encode_state_map(h, mem, per_buf) : cudaSuccess;
+    (void)per_buf;
+    return cudaSuccess;
 }
 
 int step_occupancy(int prec) {
@@ -252,21 +259,21 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
     c->desc = *d;
     c->device = dev;
     CaseDev &h = c->host;
-    case_layout(h, d->nx, d->ny, d->precision, march_default());
+    case_layout(h, d->nx, d->ny, d->precision);
     h.parity0 = 0;
     h.chunk_len = INT_MAX;
     h.aux_at_end = 0;
     fill_params(h, d->op, d->tau, d->A_fact, d->beta, d->rho_B > 0 ? d->rho_B : 1.0);
+    fill_shift(h, h.rho0, d->geometry == ITLBM_GEOM_DROP ? d->v0 : 0.0);
     const size_t elem = elem_of(d->precision);
     const size_t per_buf = (size_t)2 * planes_of(d->precision) * h.stride * elem;
     if ((e = cudaMalloc(&c->mem, 2 * per_buf)) != cudaSuccess) {
         itlbm_case_destroy(c);
         return cuda_fail(e, "cudaMalloc(state)");
     }
-    if ((e = case_bind(h, c->mem, per_buf)) != cudaSuccess ||
-        (h.march && (e = march_prepare()) != cudaSuccess)) {
+    if ((e = case_bind(h, c->mem, per_buf)) != cudaSuccess) {
         itlbm_case_destroy(c);
-        return cuda_fail(e, "state tensor map");
+        return cuda_fail(e, "state binding");
     }
     h.aux = nullptr;
     std::vector<TileRef> by_shape[NSHAPE], tl;
@@ -327,7 +334,7 @@ int itlbm_case_step(itlbm_case *c, int nsteps, int flags, void *stream) {
             const int n = c->tile_off[sh + 1] - c->tile_off[sh];
             if (n == 0) continue;
             cudaError_t e = launch_step(c->dev, c->tiles + c->tile_off[sh], n, nullptr, n, k, aux_k,
-                                        c->host.prec, c->host.march != 0, sh, s);
+                                        c->host.prec, sh, s);
             if (e != cudaSuccess) return cuda_fail(e, "step kernel");
         }
     }
@@ -341,7 +348,6 @@ int itlbm_case_sync(itlbm_case *c) {
     if (int rd = use_device(c->device)) return rd;
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "synchronize");
-    if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
     return ITLBM_OK;
 }
 

@@ -31,6 +31,7 @@
 namespace itlbm {
 void fill_params(CaseDev &c, const itlbm_operador &op, double tau, double A_fact, double beta,
                  double rho0);
+void fill_shift(CaseDev &c, double rho0, double u0x);
 }  // namespace itlbm
 
 using namespace itlbm;
@@ -124,7 +125,6 @@ struct itlbm_batch {
     // ctas_per_sm = 0 the first full replay times both tilings and keeps the faster
     bool narrow = true;
     cudaEvent_t tev[2] = {};
-    bool march = false;  // FP32 cases run the marching kernel
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // one chain of step launches per non-empty table, each on its own stream between a fork and a
@@ -219,7 +219,7 @@ cudaError_t enqueue_chain(itlbm_batch *b, int pi, int k0, int k1, cudaStream_t s
             const int p = pi * NSHAPE + sh;
             if (b->grid[p] > 0)
                 e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
-                                prec_of_table(p) == ITLBM_PREC_F32 && b->march, sh, st);
+                                sh, st);
         }
     return e;
 }
@@ -430,8 +430,9 @@ int admit_cases(itlbm_batch *b) {
         a->bytes = bytes;
         const itlbm_case_desc &d = p.desc;
         CaseDev h{};
-        case_layout(h, d.nx, d.ny, d.precision, b->march);
+        case_layout(h, d.nx, d.ny, d.precision);
         fill_params(h, d.op, d.tau, d.A_fact, d.beta, d.rho_B > 0 ? d.rho_B : 1.0);
+        fill_shift(h, h.rho0, d.geometry == ITLBM_GEOM_DROP ? d.v0 : 0.0);
         const size_t elem = elem_of(d.precision);
         const size_t per_buf = (size_t)2 * planes_of(d.precision) * h.stride * elem;
         cudaError_t e = cudaMallocFromPoolAsync(&a->mem, 2 * per_buf, b->pool, b->stream);
@@ -621,11 +622,6 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
         return cuda_fail(e, "cudaGetDevice");
     }
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
-    b->march = march_default();
-    if (b->march && (e = march_prepare()) != cudaSuccess) {
-        delete b;
-        return cuda_fail(e, "marching kernel attributes");
-    }
     if (b->cfg.hbm_budget == 0) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
@@ -865,7 +861,6 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         if (e != cudaSuccess) return cuda_fail(e, "diagnostic copy");
     }
     if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "replay");
-    if (march_error_take()) return fail(ITLBM_E_TIMEOUT, "step kernel: a copy into shared memory did not land");
     float ms = 0;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->device_ms += ms;

@@ -56,7 +56,7 @@ __device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int 
             const long long o = (long long)ys * c.pitch + xs;
             const double e = d[(long long)i * c.stride + o];
             const double dd = d[(long long)(NV + i) * c.stride + o];
-            const double f = wgt<double>(i) * c.rho0 + e;
+            const double f = (double)c.sh[i] + e;
             fR[i] = 0.5 * (f + dd);
             fB[i] = 0.5 * (f - dd);
         });
@@ -70,7 +70,7 @@ __device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int 
             const int ys = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
             const long long o = (long long)ys * c.pitch + xs;
             const double share = wgt<double>(i) / wk<double>(K);
-            const double f = (wk<double>(K) * c.rho0 + d[(long long)K * c.stride + o]) * share;
+            const double f = ((double)c.shk[K] + d[(long long)K * c.stride + o]) * share;
             const double dd = d[(long long)(NK + K) * c.stride + o] * share;
             fR[i] = 0.5 * (f + dd);
             fB[i] = 0.5 * (f - dd);

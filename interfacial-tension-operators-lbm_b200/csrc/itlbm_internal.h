@@ -28,10 +28,6 @@ constexpr int STEP_THREADS = 256;
 enum { SHAPE_32x8 = 0, SHAPE_16x16 = 1, SHAPE_8x32 = 2, NSHAPE = 3 };
 __host__ __device__ constexpr int shape_w(int s) { return s == SHAPE_32x8 ? 32 : (s == SHAPE_16x16 ? 16 : 8); }
 __host__ __device__ constexpr int shape_h(int s) { return STEP_THREADS / shape_w(s); }
-// Marching kernel of the FP32 step (itlbm_march.cu): work items are 32-column strips of MARCH_SEG rows.
-constexpr int MARCH_W = 32;
-constexpr int MARCH_SEG = 64;
-
 // D3Q19 velocity set in the order of def_lattice_d3q19 (SimBoltz_Functions/LBM_functions.cpp:366-497)
 __host__ __device__ constexpr int cx(int i) {
     constexpr int t[NV] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
@@ -95,7 +91,6 @@ __host__ __device__ __forceinline__ void sfor(F &&f) {
 
 // Per-case descriptor read by the step and diagnostic kernels (device memory).
 struct CaseDev {
-    CUtensorMap tmap;      // FP32 marching kernel: {nx, ny, 38, 2} view of both buffers (64-B aligned)
     void *buf[2];          // the two state buffers, each 2 x 19 arrays of `stride` elements
     double *aux;           // 4 arrays of pitch*ny doubles: Fx, Fy, Fz, |grad rho^N| (may be null)
     long long stride;      // elements per population array (pitch * ny)
@@ -107,8 +102,6 @@ struct CaseDev {
     int parity0;           // buffer index holding the state at sub-step k = 0
     int chunk_len;         // sub-steps to run in this launch sequence (INT_MAX for single cases)
     int aux_at_end;        // keep aux at sub-step chunk_len - 1
-    int march;             // FP32: 1 = marching kernel (work items = strips x segments), 0 = tiles
-    int m_strips, m_items; // marching kernel: strips per segment row, work items
     double A;              // amplitude (class P)
     double sigma;          // tension (class F)
     double beta;           // recolouring factor
@@ -116,12 +109,27 @@ struct CaseDev {
     double src_factor;     // 1. - 1. / (2. * tau)             (LBM_functions.cpp:1648)
     double B0, B1, B2;     // coef_B of |c|^2 = 0, 1, 2        (Operadores_tensao.cpp:94-109)
     double kf, bf;         // F3: k = 3 sigma xi / 4, b = 3 sigma / (8 xi) (Operadores_tensao.cpp:240-241)
-    double rho0;           // FP32 shifted storage: reference density of e_i = f_i - w_i rho0
+    double rho0;           // FP32 shifted storage: reference density of the shift below
+    // FP32 shifted storage: e_i = f_i - s_i with s_i the equilibrium at density rho0 and velocity
+    // U0 = (u0x, 0), the case's initial flow (a translating drop's v0 along x; zero otherwise):
+    //   s_i = w_i rho0 (1 + 3 c_ix u0x + 4.5 (c_ix u0x)^2 - 1.5 u0x^2).
+    // A uniform shift commutes with streaming, and with U0 the stored deviations stay small where the
+    // fluid moves with the drop, so their rounding stays at the scale of the deviations.  The kernels
+    // form s_i = w_i (c_ix == 0 ? s0 : sx +- j3) from three floats; sh and shk hold the same values,
+    // formed by the host with the same float operations, for import, export and the diagnostics.
+    double u0x;
+    float j0x;             // rho0 u0x
+    float u0b;             // rho0 u0x^2
+    float s0;              // rho0 (1 - 1.5 u0x^2): s_i / w_i of the directions with c_ix = 0
+    float sx;              // s0 + 4.5 rho0 u0x^2
+    float j3;              // 3 rho0 u0x
+    float sh[NV];          // s_i of each direction
+    float shk[NK];         // fold: shift of each class, the sum of its members' s_i
 };
 
 // An entry of the work table: case index and work item within that case.  For the tile kernel the
 // item is the tile's origin in units of 8 nodes, packed as ((y0 / 8) << 16) | (x0 / 8) (no division
-// in the kernel); for the marching kernel it is the linear item index.
+// in the kernel).
 struct TileRef {
     int case_id;
     int tile;
@@ -132,6 +140,9 @@ inline bool box_tileable(int nx, int ny) {
     return (nx + 7) / 8 <= MAX_TILE_COORD && (ny + 7) / 8 <= MAX_TILE_COORD;
 }
 inline int tile_code(int x0, int y0) { return (int)(((unsigned)(y0 / 8) << 16) | (unsigned)(x0 / 8)); }
+
+// The FP32 storage shift of a case: the equilibrium at density rho0 and velocity (u0x, 0).
+void fill_shift(CaseDev &c, double rho0, double u0x);
 
 // ---- kernel launchers (defined in the .cu files) -------------------------------------------
 cudaError_t launch_step_f64(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
@@ -147,29 +158,21 @@ void seam_perturb(int n, double A, double B0, double B1, double B2, const double
 void seam_source(int n, const double *F, const double *u, double factor, double *S);
 void seam_colisao(int n, const CaseDev &c, bool force, double *fR, double *fB, const double *gm,
                   const double *F);
-cudaError_t launch_march_f32(const CaseDev *cases_dev, const TileRef *items, int nitems,
-                             const int *nitems_dev, int grid, int k, int aux_k, cudaStream_t s);
-cudaError_t march_prepare();
-int march_error_take();
-cudaError_t encode_state_map(CaseDev &h, void *mem, size_t per_buf);
-size_t march_smem_bytes();
-// Layout of a case's state and its work items (tiles or marching items), and the binding of its
-// state block: pointers and, for the marching kernel, the tensor map.
-void case_layout(CaseDev &h, int nx, int ny, int prec, bool march);
-// The work items of a case with index case_id, appended to out[shape] (NSHAPE vectors): the marching kernel's items
-// (all in out[SHAPE_32x8]), or its tiles -- 32 x 8, and with narrow_edges a last partial tile column
-// of r = nx mod 32 columns cut into 8 x 32 tiles (r <= 8) or 16 x 16 tiles (8 < r <= 16).
+// Layout of a case's state and its tiles, and the binding of its state block.
+void case_layout(CaseDev &h, int nx, int ny, int prec);
+// The tiles of a case with index case_id, appended to out[shape] (NSHAPE vectors): 32 x 8, and with
+// narrow_edges a last partial tile column of r = nx mod 32 columns cut into 8 x 32 tiles (r <= 8) or
+// 16 x 16 tiles (8 < r <= 16).
 void case_tiles(const CaseDev &h, bool narrow_edges, int case_id, std::vector<TileRef> *out);
 cudaError_t case_bind(CaseDev &h, void *mem, size_t per_buf);
-// The FP32 kernel the library uses: the tile kernel, or the marching kernel with ITLBM_STEP_KERNEL=march.
-bool march_default();
-// Whether single cases cut a partial last tile column into narrow tiles (ITLBM_NARROW_EDGES=0: no).
+// Whether single cases cut a partial last tile column into narrow tiles (ITLBM_NARROW_EDGES=1): off
+// by default, since each shape is a launch of its own and a single case's steps are launch-bound
+// below about 10^6 nodes; the batch's autotuner chooses for itself.
 bool narrow_edges_default();
-// `march` selects the FP32 kernel; FP64 always runs the tile kernel; `shape` is the tile shape of
-// every entry of `tiles` (tile kernel only).
+// The step kernel of storage form `prec`; `shape` is the tile shape of every entry of `tiles`.
 cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntiles,
-                        const int *ntiles_dev, int grid, int k, int aux_k, int prec, bool march,
-                        int shape, cudaStream_t s);
+                        const int *ntiles_dev, int grid, int k, int aux_k, int prec, int shape,
+                        cudaStream_t s);
 cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
                         cudaStream_t s);  // single cases: stages the profile, waits
 size_t profile_len(const CaseDev &c, const itlbm_case_desc &d);

@@ -228,8 +228,25 @@ __device__ __forceinline__ void colisao_site_f64(double (&fR)[NV], double (&fB)[
     });
 }
 
+// The shift s of a direction (or class) with x velocity ex: w (s0 + 3 c.J0 + 4.5 (c.J0)(c.U0)), the
+// equilibrium at rho0 and U0 = (u0x, 0) (CaseDev).
+template <int ex>
+__device__ __forceinline__ float shift_of(const CaseDev &c, float w) {
+    if constexpr (ex == 0) return w * c.s0;
+    else if constexpr (ex > 0) return w * (c.sx + c.j3);
+    else return w * (c.sx - c.j3);
+}
+
 // ---------------------------------------------------------------------------------------------
-// FP32 shifted form: e_i = f_i - w_i rho0, d_i = f_R,i - f_B,i
+// FP32 shifted form: e_i = f_i - s_i, d_i = f_R,i - f_B,i, with s_i the equilibrium at the case's
+// reference density rho0 and initial flow velocity U0 (CaseDev::sh); U0 = 0 gives s_i = w_i rho0.
+// With P = rho u* (u* the velocity with half the force) and Delta = P - rho0 U0 = sum c_i e_i + F/2,
+// the equilibrium minus the shift is, per direction,
+//   f_eq,i - s_i = w_i (drho + 3 c.Delta + 4.5 ((c.P)^2 / rho - rho0 (c.U0)^2) - 1.5 (P^2 / rho - rho0 U0^2))
+// and each difference of squares is formed from the small deviations only (U0 = (u0x, 0)):
+//   (c.P)^2 / rho - rho0 (c.U0)^2 = (c.Delta (2 rho0 c.U0 + c.Delta) - drho rho0 (c.U0)^2) / rho,
+//   P^2 / rho - rho0 U0^2        = (Delta.(2 rho0 U0 + Delta) - drho rho0 U0^2) / rho,
+// so the stored values and every rounding stay at the scale of the deviations from the initial flow.
 // ---------------------------------------------------------------------------------------------
 // The FP32 form is evaluated by opposite-direction pairs: c_{2m} = -c_{2m-1} (m = 1..9), so the
 // pair shares c.u, the symmetric part of f_eq, c.F, (c.g)^2 and the recolouring term; the rest
@@ -246,7 +263,7 @@ __device__ __forceinline__ T cdotp(T a, T b, T c3) {  // c_i . (a, b, c3), non-z
     return s;
 }
 
-// Recolouring split of the FP32 form: d_i = rho^N f_i - fat2 w_i cos(phi_i) with
+// Recolouring split of the FP32 form: d_i = rho^N f_i - fat2 w_i cos(phi_i), f_i = s_i + e_i, with
 // fat2 = 2 beta c_R c_B rho = beta (1 - rho^N^2) rho / 2 (c_R - c_B = rho^N) and
 // cos(phi_i) = (c_i . g) / (|c_i| |g|); k1 and k2 fold fat2 w_i / (|c_i| |g|) of the two speeds.
 // d_0 is the complement D - sum_{i>=1} d_i, formed by the step kernel with FP64 sums.
@@ -255,18 +272,17 @@ struct Recolour32 {
     bool skip;
 };
 
-// d_i and d_{i+1} of the pair (i, i + 1), i odd, from the post-collision e_i, e_{i+1}.
+// d_i and d_{i+1} of the pair (i, i + 1), i odd, from the post-collision e_i, e_{i+1} and the shifts
+// s_i, s_{i+1}.
 template <int i>
-__device__ __forceinline__ void split32_pair(const Recolour32 &r, float ei, float ej, float rho0, float &di,
-                                             float &dj) {
-    constexpr float w = wgt<float>(i);
-    const float wr = w * rho0;
+__device__ __forceinline__ void split32_pair(const Recolour32 &r, float ei, float ej, float si, float sj,
+                                             float &di, float &dj) {
     const float K = cdotp<i>(r.gx, r.gy, r.gz) * (cc(i) == 1 ? r.k1 : r.k2);
-    di = fmaf(r.phi, wr + ei, -K);
-    dj = fmaf(r.phi, wr + ej, K);
+    di = fmaf(r.phi, si + ei, -K);
+    dj = fmaf(r.phi, sj + ej, K);
 }
 
-// e_i = f_i - w_i rho0 in, post-collision e_i out; drho = sum e_i, D = sum d_i = rho_R - rho_B.
+// e_i = f_i - s_i in, post-collision e_i out; drho = sum e_i, D = sum d_i = rho_R - rho_B.
 template <bool FORCE>
 __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D, float gmx,
                                             float gmy, float gmz, float Fx, float Fy, float Fz,
@@ -294,26 +310,32 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
         if constexpr (cz(i) == 1) jz += p;
         if constexpr (cz(i) == -1) jz -= p;
     });
-    const float vx = fmaf(jx, inv_rho, 0.5f * ax), vy = fmaf(jy, inv_rho, 0.5f * ay);
-    const float vz = fmaf(jz, inv_rho, 0.5f * az);
-    const float usq15 = 1.5f * (vx * vx + vy * vy + vz * vz);
+    // Delta = sum c_i e_i + F / 2 and the velocity u* = (rho0 U0 + Delta) / rho
+    const float Dx = FORCE ? fmaf(0.5f, Fx, jx) : jx, Dy = FORCE ? fmaf(0.5f, Fy, jy) : jy;
+    const float Dz = FORCE ? fmaf(0.5f, Fz, jz) : jz;
+    const float vx = (c.j0x + Dx) * inv_rho, vy = Dy * inv_rho, vz = Dz * inv_rho;
+    const float s15 = 1.5f * inv_rho, s45 = 4.5f * inv_rho;
+    const float usq15 = s15 * (fmaf(Dx, fmaf(2.0f, c.j0x, Dx), fmaf(Dy, Dy, Dz * Dz)) - drho * c.u0b);
     const float inv_tau = (float)c.inv_tau;
-    const float rho3 = 3.0f * rho;
     const float Frx = ax * rho, Fry = ay * rho, Frz = az * rho;
     const float vF = Frx * vx + Fry * vy + Frz * vz;
     const float fac3 = 3.0f * (float)c.src_factor;
-    // BGK (+ Guo source) of the moving populations:
-    //   f_eq - w rho0 = w (drho + rho (4.5 cu^2 - 1.5 u^2) +- 3 rho cu)
+    // BGK (+ Guo source) of the moving populations, pair (i, j) with c_j = -c_i, d = c_i.Delta:
+    //   f_eq - s = w (drho + 4.5 (d (a + d) - drho b) / rho - usq15 +- 3 d),  a = 2 rho0 c.U0, b = rho0 (c.U0)^2
     //   S = 3 (1 - 1/2tau) w (3 (c.F)(c.u) - u.F +- c.F)
     sfor<0, 9>([&](auto M) {
         constexpr int i = 2 * decltype(M)::value + 1;
         constexpr float w = wgt<float>(i);
-        const float cu = cdotp<i>(vx, vy, vz);
-        const float sym = w * fmaf(rho, fmaf(4.5f * cu, cu, -usq15), drho);
-        const float asym = (w * rho3) * cu;
+        const float cD = cdotp<i>(Dx, Dy, Dz);
+        float q;  // (c.Delta) (2 rho0 c.U0 + c.Delta) - drho rho0 (c.U0)^2
+        if constexpr (cx(i) == 0) q = cD * cD;
+        else q = fmaf(cD, fmaf(cx(i) > 0 ? 2.0f : -2.0f, c.j0x, cD), -drho * c.u0b);
+        const float sym = w * fmaf(s45, q, drho - usq15);
+        const float asym = (3.0f * w) * cD;
         float ei = fmaf((sym + asym) - e[i], inv_tau, e[i]);
         float ej = fmaf((sym - asym) - e[i + 1], inv_tau, e[i + 1]);
         if constexpr (FORCE) {
+            const float cu = cdotp<i>(vx, vy, vz);
             const float cF = cdotp<i>(Frx, Fry, Frz);
             const float P = fmaf(3.0f * cF, cu, -vF);
             ei = fmaf(fac3 * w, P + cF, ei);
@@ -382,17 +404,18 @@ struct RecolourFold {
     bool skip;
 };
 
-// d_K and d_{K+1} of the class pair (K, K + 1), K odd, from the post-collision e_K, e_{K+1}.
+// d_K and d_{K+1} of the class pair (K, K + 1), K odd, from the post-collision e_K, e_{K+1} and the
+// class shifts s_K, s_{K+1}.
 template <int K>
-__device__ __forceinline__ void split_fold_pair(const RecolourFold &r, float eK, float eJ, float rho0, float &dK,
-                                                float &dJ) {
-    const float wr = wk<float>(K) * rho0;
+__device__ __forceinline__ void split_fold_pair(const RecolourFold &r, float eK, float eJ, float sK, float sJ,
+                                                float &dK, float &dJ) {
     const float A = kdot<K>(r.gx, r.gy) * (kk(K) == 1 ? r.k1 : r.k2);
-    dK = fmaf(r.phi, wr + eK, -A);
-    dJ = fmaf(r.phi, wr + eJ, A);
+    dK = fmaf(r.phi, sK + eK, -A);
+    dJ = fmaf(r.phi, sJ + eJ, A);
 }
 
-// e_K = F_K - W_K rho0 of the nine classes in, post-collision out; drho = sum e_K, D = sum d_K.
+// e_K = F_K - s_K of the nine classes in (s_K the class sum of the shifts s_i), post-collision out;
+// drho = sum e_K, D = sum d_K.  The equilibrium is formed from the deviations as in collide_f32.
 template <bool FORCE>
 __device__ __forceinline__ void collide_fold(float (&e)[NK], float drho, float D, float gmx, float gmy,
                                              float Fx, float Fy, const CaseDev &c, RecolourFold &rc) {
@@ -416,22 +439,27 @@ __device__ __forceinline__ void collide_fold(float (&e)[NK], float drho, float D
         if constexpr (ky(K) == 1) jy += p;
         if constexpr (ky(K) == -1) jy -= p;
     });
-    const float vx = fmaf(jx, inv_rho, 0.5f * ax), vy = fmaf(jy, inv_rho, 0.5f * ay);
-    const float usq15 = 1.5f * (vx * vx + vy * vy);
+    const float Dx = FORCE ? fmaf(0.5f, Fx, jx) : jx, Dy = FORCE ? fmaf(0.5f, Fy, jy) : jy;
+    const float vx = (c.j0x + Dx) * inv_rho, vy = Dy * inv_rho;
+    const float s15 = 1.5f * inv_rho, s45 = 4.5f * inv_rho;
+    const float usq15 = s15 * (fmaf(Dx, fmaf(2.0f, c.j0x, Dx), Dy * Dy) - drho * c.u0b);
     const float inv_tau = (float)c.inv_tau;
-    const float rho3 = 3.0f * rho;
     const float Frx = ax * rho, Fry = ay * rho;
     const float vF = Frx * vx + Fry * vy;
     const float fac3 = 3.0f * (float)c.src_factor;
     sfor<0, 4>([&](auto M) {
         constexpr int K = 2 * decltype(M)::value + 1;
         constexpr float W = wk<float>(K);
-        const float cu = kdot<K>(vx, vy);
-        const float sym = W * fmaf(rho, fmaf(4.5f * cu, cu, -usq15), drho);
-        const float asym = (W * rho3) * cu;
+        const float cD = kdot<K>(Dx, Dy);
+        float q;
+        if constexpr (kx(K) == 0) q = cD * cD;
+        else q = fmaf(cD, fmaf(kx(K) > 0 ? 2.0f : -2.0f, c.j0x, cD), -drho * c.u0b);
+        const float sym = W * fmaf(s45, q, drho - usq15);
+        const float asym = (3.0f * W) * cD;
         float eK = fmaf((sym + asym) - e[K], inv_tau, e[K]);
         float eJ = fmaf((sym - asym) - e[K + 1], inv_tau, e[K + 1]);
         if constexpr (FORCE) {
+            const float cu = kdot<K>(vx, vy);
             const float cF = kdot<K>(Frx, Fry);
             const float P = fmaf(3.0f * cF, cu, -vF);
             eK = fmaf(fac3 * W, P + cF, eK);
@@ -554,8 +582,8 @@ __device__ __forceinline__ float chem_pot_fold(P phi, float kf, float bf) {
 // ---------------------------------------------------------------------------------------------
 
 // The stencils below read the staged phase field through an accessor P(dx, dy) = rho^N at
-// (x + dx, y + dy), so that the tile kernel (a plain 2-D array) and the marching kernel (a ring of
-// rows) evaluate them with the same arithmetic in the same order.
+// (x + dx, y + dy), so that every tile shape (a plain 2-D array of its own width) and the per-site
+// seam evaluate them with the same arithmetic in the same order.
 
 // Mediator momentum at the node: sum_i c_i * (w_i * (phi(x - c_i) * 3)), the momentum()
 // (LBM_functions.cpp:1057-1087) of the mediators after emite_mediadores + propag_site_med

@@ -22,7 +22,7 @@ constexpr char MAGIC[8] = {'I', 'T', 'L', 'B', 'M', 'S', 'T', '1'};
 int snap_write(const char *path, const itlbm_case_desc &d, long long steps, const CaseDev &h, const void *state) {
     SnapHeader hd{};
     std::memcpy(hd.magic, MAGIC, 8);
-    hd.version = 1;
+    hd.version = 2;  // 2: FP32 states are deviations from the equilibrium at the case's initial flow
     hd.desc = d;
     hd.steps = steps;
     const size_t elem = elem_of(h.prec), row = elem * (size_t)h.nx;
@@ -48,7 +48,7 @@ int snap_read_header(const char *path, SnapHeader &hd) {
     if (!f) return fail(ITLBM_E_IO, std::string("cannot open ") + path);
     const bool ok = std::fread(&hd, sizeof hd, 1, f) == 1;
     std::fclose(f);
-    if (!ok || std::memcmp(hd.magic, MAGIC, 8) != 0 || hd.version != 1)
+    if (!ok || std::memcmp(hd.magic, MAGIC, 8) != 0 || hd.version != 2)
         return fail(ITLBM_E_PARSE, std::string("not a case snapshot: ") + path);
     const itlbm_case_desc &d = hd.desc;
     if (d.nx < 1 || d.ny < 1 || (long long)d.nx * d.ny > (1LL << 30) || hd.steps < 0 ||

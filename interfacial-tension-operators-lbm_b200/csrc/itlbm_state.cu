@@ -32,8 +32,7 @@ __device__ void store_state(const CaseDev &c, int buf, long long off, const doub
     } else if (c.prec == ITLBM_PREC_F32) {
         float *d = (float *)c.buf[buf];
         for (int i = 0; i < NV; i++) {
-            const double wr = wgt<double>(i) * c.rho0;
-            d[(long long)i * c.stride + off] = (float)((fR[i] + fB[i]) - wr);
+            d[(long long)i * c.stride + off] = (float)((fR[i] + fB[i]) - (double)c.sh[i]);
             d[(long long)(NV + i) * c.stride + off] = (float)(fR[i] - fB[i]);
         }
     } else {  // fold: class sums of the members (FP64), then shifted and rounded
@@ -44,7 +43,7 @@ __device__ void store_state(const CaseDev &c, int buf, long long off, const doub
             Dk[fold_class(i)] += fR[i] - fB[i];
         }
         for (int K = 0; K < NK; K++) {
-            d[(long long)K * c.stride + off] = (float)(F[K] - wk<double>(K) * c.rho0);
+            d[(long long)K * c.stride + off] = (float)(F[K] - (double)c.shk[K]);
             d[(long long)(NK + K) * c.stride + off] = (float)Dk[K];
         }
     }
@@ -52,9 +51,9 @@ __device__ void store_state(const CaseDev &c, int buf, long long off, const doub
 
 // The 19 populations of a node of the fold: each class split among its members by weight (exact
 // for the class sums and every moment; a member's own share is that of the split).
-__device__ __forceinline__ void unfold_split(double E, double D, int K, int i, double rho0, double &fR, double &fB) {
+__device__ __forceinline__ void unfold_split(double E, double D, int K, int i, double sK, double &fR, double &fB) {
     const double share = wgt<double>(i) / wk<double>(K);
-    const double f = (wk<double>(K) * rho0 + E) * share, d = D * share;
+    const double f = (sK + E) * share, d = D * share;
     fR = 0.5 * (f + d);
     fB = 0.5 * (f - d);
 }
@@ -127,7 +126,7 @@ __global__ void k_export(const CaseDev *__restrict__ cp, int cur, int which, dou
                 const long long off = (long long)ys * c.pitch + xs;
                 const float *d = (const float *)c.buf[cur];
                 unfold_split(d[(long long)K * c.stride + off], d[(long long)(NK + K) * c.stride + off], K, i,
-                             c.rho0, r, b);
+                             (double)c.shk[K], r, b);
                 oR[t * NV + i] = r;
                 oB[t * NV + i] = b;
                 continue;
@@ -141,7 +140,7 @@ __global__ void k_export(const CaseDev *__restrict__ cp, int cur, int which, dou
                 const float *d = (const float *)c.buf[cur];
                 const double e = d[(long long)i * c.stride + off];
                 const double dd = d[(long long)(NV + i) * c.stride + off];
-                const double f = wgt<double>(i) * c.rho0 + e;
+                const double f = (double)c.sh[i] + e;
                 r = 0.5 * (f + dd);
                 b = 0.5 * (f - dd);
             }

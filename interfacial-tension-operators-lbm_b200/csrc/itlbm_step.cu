@@ -308,12 +308,12 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             else collide_fold<false>(f, sa, sb, gmx, gmy, Fx, Fy, c, rc);
             skip = rc.skip;
             if (!skip) {
-                const float rho0 = (float)c.rho0;
                 double dsum = 0.0;
                 sfor<0, 4>([&](auto M) {
                     constexpr int K = 2 * decltype(M)::value + 1;
                     float dK, dJ;
-                    split_fold_pair<K>(rc, f[K], f[K + 1], rho0, dK, dJ);
+                    split_fold_pair<K>(rc, f[K], f[K + 1], shift_of<kx(K)>(c, wk<float>(K)),
+                                       shift_of<kx(K + 1)>(c, wk<float>(K + 1)), dK, dJ);
                     dsum += (double)dK;
                     dsum += (double)dJ;
                     const int oK = dst_off(K), oJ = dst_off(K + 1);
@@ -351,12 +351,12 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                 // FP64: the d_i are O(w_i rho), so FP32 sums would round by ~1e-8 rho per node and
                 // step, coherently over uniform regions, and drift the colour masses (1e-6 in 2000
                 // steps); in FP64 the only rounding left is that of d_0 itself.
-                const float rho0 = (float)c.rho0;
                 double dsum = 0.0;
                 sfor<0, 9>([&](auto M) {
                     constexpr int i = 2 * decltype(M)::value + 1;
                     float di, dj;
-                    split32_pair<i>(rc, f[i], f[i + 1], rho0, di, dj);
+                    split32_pair<i>(rc, f[i], f[i + 1], shift_of<cx(i)>(c, wgt<float>(i)),
+                                    shift_of<cx(i + 1)>(c, wgt<float>(i + 1)), di, dj);
                     dsum += (double)di;
                     dsum += (double)dj;
                     const int oi = dst_off(i), oj = dst_off(i + 1);

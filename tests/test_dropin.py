@@ -226,8 +226,21 @@ def test_unstable_case_is_reported_not_failed(tmp_path):
 # whose value is round-off (stated per column).
 needs_strict = pytest.mark.skipif(not (REF / "Imm_OPS_strict").exists(), reason="oracle/_ref not built")
 
-LAP_FLOORS = {13: 1e-12, 14: 1e-9, 15: 1e-9, 8: 1e-15, 9: 1e-15, 10: 1e-13}  # |q|, sd_p_in/out, |u|, Ca
+# laplace.dat columns (0-based) whose value is round-off somewhere in a run: delta_p, sigma and
+# sigma_2pontos of the initial state (zero up to cancellation), |q| (a sum of momenta that cancels),
+# sd_p_in / sd_p_out (sqrt(E[p^2] - E[p]^2) of a uniform pressure: the square root of a cancellation,
+# up to ~1e-6 for sums over 10^4 nodes in different orders), |u|
+LAP_FLOORS = {6: 1e-12, 7: 1e-12, 16: 1e-12, 13: 1e-12, 14: 1e-6, 15: 1e-6, 8: 1e-15, 9: 1e-15}
 LAP_SHELL = (17, 18, 19, 20, 21)  # the shell fit of calc_perfil_logistico (a node at r = k/2 flips shell)
+LAP_CA = 10  # Ca = nu u_max / sigma: compared only where sigma is not round-off
+
+
+def compare_ca(a, b):
+    bad = []
+    for i, (x, y) in enumerate(zip(_rows(a), _rows(b))):
+        if abs(float(y[7])) > 1e-10 and abs(float(x[LAP_CA]) - float(y[LAP_CA])) > 1e-9 * abs(float(y[LAP_CA])):
+            bad.append((i, x[LAP_CA], y[LAP_CA]))
+    return bad
 GI_FLOORS = {k: 1e-12 for k in range(1, 36)}
 
 
@@ -249,7 +262,8 @@ def test_itlbm_ops_matches_strict_imm_ops(tmp_path, oper, A, v0):
     assert ra.returncode == rb.returncode == 0, ra.stderr[-800:]
     for f in ("rho_R1000.vtk", "rho_B1000.vtk", "vel_1000.vtk"):
         assert (a / f).read_bytes() == (b / f).read_bytes(), f
-    assert not compare_tight(a / "laplace.dat", b / "laplace.dat", LAP_FLOORS, skip=LAP_SHELL)
+    assert not compare_tight(a / "laplace.dat", b / "laplace.dat", LAP_FLOORS, skip=LAP_SHELL + (LAP_CA,))
+    assert not compare_ca(a / "laplace.dat", b / "laplace.dat")
     assert not compare_files(a / "laplace.dat", b / "laplace.dat", skip_cols=tuple(range(17)), rel=2e-2)
     assert not compare_tight(a / "iso.dat", b / "iso.dat", {2: 1e-9, 3: 1e-9, 4: 1e-9})
     assert not compare_tight(a / "galilean.dat", b / "galilean.dat", GI_FLOORS, rel=1e-8)
@@ -265,6 +279,7 @@ def test_itlbm_incl_matches_strict_imm_incl(tmp_path, oper, A, pq):
     rb = run(REF / "Imm_INCL_strict", b)
     assert ra.returncode == rb.returncode == 0, ra.stderr[-800:]
     assert (a / "perfil.dat").read_bytes() == (b / "perfil.dat").read_bytes()
-    # 7 d0, 14-17 net momentum / force sums: round-off
-    assert not compare_tight(a / "inclinada.dat", b / "inclinada.dat", {6: 1e-9, 13: 1e-12, 14: 1e-12, 15: 1e-12,
-                                                                         16: 1e-12, 17: 1e-16})
+    # round-off columns: 2 sigma_pop of a flat interface at rest, 6 the largest fit residual, 7 d0,
+    # 14-17 net momentum / force sums, 18 min_f
+    assert not compare_tight(a / "inclinada.dat", b / "inclinada.dat", {1: 1e-14, 5: 1e-12, 6: 1e-9, 13: 1e-12,
+                                                                         14: 1e-12, 15: 1e-12, 16: 1e-12, 17: 1e-16})

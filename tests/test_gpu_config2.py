@@ -15,7 +15,7 @@ import math
 import numpy as np
 import pytest
 
-from test_gpu_parity import OPS, OP_IDS, close_diag, gpu_case, maxdiff, same
+from test_gpu_parity import OPS, OP_IDS, SHELL_FIT, close_diag, gpu_case, maxdiff, same
 
 pytestmark = pytest.mark.gpu
 
@@ -64,7 +64,9 @@ def test_config2_30000_steps(gpu, oracle):
         o.step(n)
         g, r = c.diag_drop(s).as_dict(), o.diag_drop(s).as_dict()
         assert g["ok"] == r["ok"] == 1, s
-        bad = close_diag(g, r)
+        # step 0 of a sharp initial step: the logistic shell fit has one usable shell or none, decided by
+        # the last bit of the centroid
+        bad = close_diag(g, r, skip=SHELL_FIT if s == 0 else ())
         assert not bad, (s, bad)
         for k in ("raio", "p_in", "p_out", "delta_p", "sigma", "u_max", "u_rms", "R0"):
             if r[k] != 0:

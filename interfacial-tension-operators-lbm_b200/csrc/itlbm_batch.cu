@@ -460,7 +460,10 @@ int admit_cases(itlbm_batch *b) {
         b->h_cases[slot] = h;
         // on the batch stream, which is not ordered after the legacy stream's copies
         e = cudaMemcpyAsync(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream);
-        if (p.snapshot.empty()) {
+        if (p.snapshot.empty() && profile_on_device(d)) {
+            if (e == cudaSuccess) e = launch_init_from(h, b->d_cases + slot, d, nullptr, b->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "admission");
+        } else if (p.snapshot.empty()) {
             const size_t len = profile_len(h, d);
             // a full staging buffer is reused only after the profiles queued in it are launched
             if (e == cudaSuccess && b->stage_used + len > b->stage_cap) e = flush_inits(b);

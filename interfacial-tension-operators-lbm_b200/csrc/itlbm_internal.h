@@ -176,6 +176,7 @@ cudaError_t launch_step(const CaseDev *cases_dev, const TileRef *tiles, int ntil
 cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
                         cudaStream_t s);  // single cases: stages the profile, waits
 size_t profile_len(const CaseDev &c, const itlbm_case_desc &d);
+bool profile_on_device(const itlbm_case_desc &d);  // FP32 drops: the init kernel evaluates the profile
 void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof);  // host, profile_len values
 void init_profile_rows(const CaseDev &c, const itlbm_case_desc &d, double *prof, int ya, int yb);
 cudaError_t launch_init_from(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,

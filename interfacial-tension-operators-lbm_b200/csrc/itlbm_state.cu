@@ -74,8 +74,10 @@ __device__ void dist_eq_dev(double *feq, double vx, double vy, double vz, double
 // f_R = dist_eq(v0, phi rho_tot), f_B = dist_eq(v0, (1 - phi) rho_tot).
 // The logistic strip of Imm_INCL.cpp:309-334, given c_R(s) for s = (p x + q y) mod N:
 // f_R = w_i c_R, f_B = w_i (1 - c_R).
+// With prof == nullptr (FP32 storage forms only) the drop's profile is evaluated here with the
+// device's sqrt and exp: within an ulp or two of the host's libm in FP64, and rounded to FP32 anyway.
 __global__ void k_init(const CaseDev *__restrict__ cp, int geometry, const double *__restrict__ prof,
-                       double v0, double rho_Ri, double rho_Bi, int p, int q) {
+                       double v0, double rho_Ri, double rho_Bi, int p, int q, double radius, double k_perfil) {
     const CaseDev &c = *cp;
     const long long n = (long long)c.nx * c.ny;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -83,7 +85,21 @@ __global__ void k_init(const CaseDev *__restrict__ cp, int geometry, const doubl
         const int x = (int)(t % c.nx), y = (int)(t / c.nx);
         double fR[NV], fB[NV];
         if (geometry == ITLBM_GEOM_DROP) {
-            const double phi = prof[t];
+            double phi;
+            if (prof) {
+                phi = prof[t];
+            } else {  // the expressions of init_profile_rows
+                const double dx = (double)(x - c.nx / 2), dy = (double)(y - c.ny / 2), dz = 0.0;
+                const double r = sqrt(dx * dx + dy * dy + dz * dz);
+                if (k_perfil > 0.0) {
+                    double arg = k_perfil * (r - radius);
+                    if (arg > 60.0) arg = 60.0;
+                    if (arg < -60.0) arg = -60.0;
+                    phi = 1.0 / (1.0 + exp(arg));
+                } else {
+                    phi = (r < radius) ? 1.0 : 0.0;
+                }
+            }
             const double rho_tot = rho_Bi + phi * (rho_Ri - rho_Bi) + phi * 0.0;
             dist_eq_dev(fR, v0, 0., 0., phi * rho_tot);
             dist_eq_dev(fB, v0, 0., 0., (1.0 - phi) * rho_tot);
@@ -228,18 +244,32 @@ void init_profile(const CaseDev &c, const itlbm_case_desc &d, double *prof) {
     for (auto &th : pool) th.join();
 }
 
+// Whether a case's initial profile is evaluated on the device: drops in the FP32 storage forms (an FP64
+// state must be the reference's to the bit, and takes its profile from the host's libm).
+bool profile_on_device(const itlbm_case_desc &d) {
+    return d.geometry == ITLBM_GEOM_DROP && d.precision != ITLBM_PREC_F64;
+}
+
 // The initial state from a profile already in memory the device can read (device memory, or
-// mapped pinned host memory, which the kernel reads across the host link once per value).
+// mapped pinned host memory, which the kernel reads across the host link once per value), or, with
+// prof == nullptr for a case with profile_on_device, from the profile evaluated by the kernel.
 cudaError_t launch_init_from(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
                              const double *prof, cudaStream_t s) {
     const long long n = (long long)c.nx * c.ny;
-    k_init<<<grid_for(n, 256), 256, 0, s>>>(c_dev, d.geometry, prof, d.v0, d.rho_R, d.rho_B, d.p, d.q);
+    const double radius = d.radius > 0.0 ? d.radius : 0.25 * (double)d.nx;
+    k_init<<<grid_for(n, 256), 256, 0, s>>>(c_dev, d.geometry, prof, d.v0, d.rho_R, d.rho_B, d.p, d.q, radius,
+                                            d.k_profile);
     return cudaGetLastError();
 }
 
-// Single cases: the profile is staged through device memory and the call waits for the state.
+// Single cases: the profile is staged through device memory (or evaluated by the kernel) and the call
+// waits for the state.
 cudaError_t launch_init(const CaseDev &c, const CaseDev *c_dev, const itlbm_case_desc &d,
                         cudaStream_t s) {
+    if (profile_on_device(d)) {
+        const cudaError_t e = launch_init_from(c, c_dev, d, nullptr, s);
+        return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+    }
     std::vector<double> prof(profile_len(c, d));
     init_profile(c, d, prof.data());
     double *dprof = nullptr;

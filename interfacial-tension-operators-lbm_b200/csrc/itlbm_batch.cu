@@ -23,6 +23,7 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <thread>
@@ -122,8 +123,10 @@ struct itlbm_batch {
     int mode = -1;
     bool tuning = false;
     // a partial last tile column of a case in narrow tiles (16 x 16, 8 x 32) instead of 32 x 8; with
-    // ctas_per_sm = 0 the first full replay times both tilings and keeps the faster
-    bool narrow = true;
+    // ctas_per_sm = 0 the first full replay times both tilings and keeps the faster (on the measured
+    // mixes 32 x 8 throughout, which is also the tiling without autotuning)
+    bool narrow = false;
+    bool tile_fixed = false;  // the tiling was set by the caller, not timed
     cudaEvent_t tev[2] = {};
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -131,6 +134,10 @@ struct itlbm_batch {
     // join on `stream`: the tables hold different cases, so their steps need no order between them
     cudaStream_t side[NPREC] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[NPREC] = {};
+    // within one storage form, the narrow-tile tables run on streams of their own beside the 32 x 8
+    // table, each sub-step after every shape's previous sub-step (events shape_ev)
+    cudaStream_t shape_st[NPREC][NSHAPE] = {};
+    cudaEvent_t shape_ev[NPREC][NSHAPE] = {}, shape_fork[NPREC] = {};
     // diagnostics: the cases that fall due in an advance are measured together, drops and strips each
     // by one sequence of launches over a table of jobs, their scratch in per-case segments of one
     // block (grown on demand, up to DIAG_SCRATCH_LIMIT or the largest single case; more due cases than
@@ -209,18 +216,46 @@ int upload_tables(itlbm_batch *b) {
     return cudaStreamSynchronize(b->stream) == cudaSuccess ? ITLBM_OK : cuda_fail(cudaGetLastError(), "sync");
 }
 
-// Sub-steps [k0, k1) of the tables of storage form pi on stream st.  The tables of one storage form
-// (one per tile shape) hold tiles of the same cases, so every sub-step launches them in turn on the
-// one stream: sub-step k of every tile of a case ends before any tile of it starts sub-step k + 1.
+// Sub-steps [k0, k1) of the tables of storage form pi, from stream st.  The tables of one storage form
+// (one per tile shape) hold tiles of the same cases: sub-step k of every tile of a case must end before
+// any tile of it starts sub-step k + 1 (which reads what k wrote and overwrites what k read).  A
+// single table runs in line on st; several run side by side, the 32 x 8 table on st and each narrow
+// table on a stream of its own, every launch of sub-step k > k0 waiting for the other shapes'
+// launches of sub-step k - 1, so that the small narrow-tile launches overlap the large one.
 cudaError_t enqueue_chain(itlbm_batch *b, int pi, int k0, int k1, cudaStream_t st) {
+    int shapes[NSHAPE], n = 0;
+    for (int sh = 0; sh < NSHAPE; sh++)
+        if (b->grid[pi * NSHAPE + sh] > 0) shapes[n++] = sh;
+    auto launch = [&](int sh, int k, cudaStream_t on) {
+        const int p = pi * NSHAPE + sh;
+        return launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
+                           sh, on);
+    };
     cudaError_t e = cudaSuccess;
-    for (int k = k0; k < k1 && e == cudaSuccess; k++)
-        for (int sh = 0; sh < NSHAPE && e == cudaSuccess; sh++) {
-            const int p = pi * NSHAPE + sh;
-            if (b->grid[p] > 0)
-                e = launch_step(b->d_cases, b->d_tiles[p], 0, b->d_ntiles + p, b->grid[p], k, -1, prec_of_table(p),
-                                sh, st);
+    if (n == 1) {
+        for (int k = k0; k < k1 && e == cudaSuccess; k++) e = launch(shapes[0], k, st);
+        return e;
+    }
+    auto stream_of = [&](int sh) { return sh == SHAPE_32x8 ? st : b->shape_st[pi][sh]; };
+    if ((e = cudaEventRecord(b->shape_fork[pi], st)) != cudaSuccess) return e;
+    for (int j = 0; j < n; j++)
+        if (shapes[j] != SHAPE_32x8 && (e = cudaStreamWaitEvent(stream_of(shapes[j]), b->shape_fork[pi], 0)) != cudaSuccess)
+            return e;
+    for (int k = k0; k < k1; k++) {
+        if (k > k0)  // every wait of sub-step k first: each names the other shapes' records of k - 1
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++)
+                    if (i != j && (e = cudaStreamWaitEvent(stream_of(shapes[j]), b->shape_ev[pi][shapes[i]], 0)) !=
+                                      cudaSuccess)
+                        return e;
+        for (int j = 0; j < n; j++) {
+            if ((e = launch(shapes[j], k, stream_of(shapes[j]))) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(b->shape_ev[pi][shapes[j]], stream_of(shapes[j]))) != cudaSuccess) return e;
         }
+    }
+    for (int j = 0; j < n; j++)
+        if (shapes[j] != SHAPE_32x8 && (e = cudaStreamWaitEvent(st, b->shape_ev[pi][shapes[j]], 0)) != cudaSuccess)
+            return e;
     return e;
 }
 
@@ -319,9 +354,15 @@ int tune_and_run(itlbm_batch *b, int K) {
     };
     double r_narrow = 0, r_uniform = 0, r_persist = 0;
     int r;
-    if ((r = window(-1, true, r_narrow)) != ITLBM_OK || (r = window(-1, false, r_uniform)) != ITLBM_OK)
-        return r;
-    const bool narrow = r_narrow >= r_uniform;
+    bool narrow = b->narrow;
+    if (!b->tile_fixed) {
+        if ((r = window(-1, true, r_narrow)) != ITLBM_OK || (r = window(-1, false, r_uniform)) != ITLBM_OK)
+            return r;
+        narrow = r_narrow >= r_uniform;
+    } else {
+        if ((r = window(-1, narrow, r_narrow)) != ITLBM_OK) return r;
+        r_uniform = r_narrow;
+    }
     if ((r = window(0, narrow, r_persist)) != ITLBM_OK) return r;
     // persistent CTAs only when clearly faster (the two are within noise on small tables)
     const int mode = r_persist > 1.02 * std::max(r_narrow, r_uniform) ? 0 : -1;
@@ -648,6 +689,13 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
     // measures faster
     b->mode = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm : -1;
     b->tuning = b->cfg.ctas_per_sm == 0;
+    // ITLBM_BATCH_TILING=narrow | uniform fixes the tiling instead of timing it
+    if (const char *v = getenv("ITLBM_BATCH_TILING")) {
+        if (!strcmp(v, "narrow") || !strcmp(v, "uniform")) {
+            b->narrow = !strcmp(v, "narrow");
+            b->tile_fixed = true;
+        }
+    }
     for (int p = 0; p < NTAB; p++) b->occ[p] = step_occupancy(prec_of_table(p));
     const int M = b->cfg.max_cases;
     b->slots.assign(M, nullptr);
@@ -683,6 +731,19 @@ int itlbm_batch_create(const itlbm_batch_config *cfg, itlbm_batch **out) {
     if ((e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess) {
         itlbm_batch_destroy(b);
         return cuda_fail(e, "batch events");
+    }
+    for (int p = 0; p < NPREC; p++) {
+        for (int sh = 0; sh < NSHAPE; sh++)
+            if ((sh != SHAPE_32x8 &&
+                 (e = cudaStreamCreateWithFlags(&b->shape_st[p][sh], cudaStreamNonBlocking)) != cudaSuccess) ||
+                (e = cudaEventCreateWithFlags(&b->shape_ev[p][sh], cudaEventDisableTiming)) != cudaSuccess) {
+                itlbm_batch_destroy(b);
+                return cuda_fail(e, "batch streams");
+            }
+        if ((e = cudaEventCreateWithFlags(&b->shape_fork[p], cudaEventDisableTiming)) != cudaSuccess) {
+            itlbm_batch_destroy(b);
+            return cuda_fail(e, "batch streams");
+        }
     }
     for (int p = 0; p < NPREC; p++)
         if ((e = cudaStreamCreateWithFlags(&b->side[p], cudaStreamNonBlocking)) != cudaSuccess ||
@@ -734,6 +795,11 @@ void itlbm_batch_destroy(itlbm_batch *b) {
     for (int p = 0; p < NPREC; p++) {
         if (b->ev_join[p]) cudaEventDestroy(b->ev_join[p]);
         if (b->side[p]) cudaStreamDestroy(b->side[p]);
+        if (b->shape_fork[p]) cudaEventDestroy(b->shape_fork[p]);
+        for (int sh = 0; sh < NSHAPE; sh++) {
+            if (b->shape_ev[p][sh]) cudaEventDestroy(b->shape_ev[p][sh]);
+            if (b->shape_st[p][sh]) cudaStreamDestroy(b->shape_st[p][sh]);
+        }
     }
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->pool) cudaMemPoolDestroy(b->pool);

@@ -13,7 +13,7 @@ measured tension sigma = R delta_p (Other_functions.cpp:530-553), the peak spuri
 (Galilean_diagnostics.cpp:93-95) and the interface mode amplitudes |a2|, |a4|, |a8| / R0
 (Operadores_tensao.cpp:382-449).  Bars, for every operator and both FP32 forms: delta_p within 0.5 %,
 peak spurious velocity within 5 %; the other errors are stated (printed, and written as JSON to
-$ITLBM_REPORT_DIR/fp32_errors.json when that variable is set) with the bounds asserted below.
+$ITLBM_REPORT_DIR/fp32_errors.json when that variable is set) with the bounds asserted in check().
 """
 import json
 import math
@@ -85,14 +85,17 @@ def record(row):
 
 
 def check(worst):
+    """The bars: the Laplace jump and the peak spurious velocity as the path's specification states them
+    (0.5 %, 5 %); the other observables at a few times their largest error measured on B200 (delta_p
+    6e-5, sigma 6e-5, radius 1e-6, slip 0.014 lattice units, |a_k| / R0 2.5e-5)."""
     for label, w in worst.items():
         assert w["delta_p"] <= 5e-3, (label, w)
         assert w["u_max"] <= 0.05, (label, w)
         assert w["sigma"] <= 5e-3, (label, w)
-        assert w["raio"] <= 1e-3, (label, w)
+        assert w["raio"] <= 1e-5, (label, w)
         assert w["slip"] <= 0.05, (label, w)  # lattice units, after up to 5 000 of travel
         for k in ("a2", "a4", "a8"):
-            assert w[k] <= 1e-3, (label, k, w)
+            assert w[k] <= 1e-4, (label, k, w)
 
 
 @pytest.mark.parametrize("name,tipo,chi,xi", OPERATORS, ids=[o[0] for o in OPERATORS])

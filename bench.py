@@ -63,9 +63,9 @@ def load_package():
 
 PEAKS = REPO / "MEASURED_PEAKS.json"
 # HBM traffic per node of one FP32 step launch, dram__bytes_read.sum + dram__bytes_write.sum from one
-# ncu capture each: a launch over the 600-case batch (12.41 GB for 39 127 049 nodes) and a launch over
-# the 4096^2 drop (5.07 GB for 16 777 216 nodes).
-TRAFFIC_B_PER_NODE = {"batch600": 12406304768 / 39127049, "single": 5069217280 / 16777216}
+# ncu capture each: a launch over a 100-case subset of the batch mix (1.73 GB for 5 542 507 nodes) and a
+# launch over the 4096^2 drop (5.07 GB for 16 777 216 nodes).
+TRAFFIC_B_PER_NODE = {"batch600": (912097536 + 816680704) / 5542507, "single": 5069217280 / 16777216}
 HBM_FALLBACK = 6650.0
 
 
@@ -790,7 +790,7 @@ def main():
                          "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_lu": 304.0,
                          "traffic": TRAFFIC_B_PER_NODE["batch600" if args.workload == "batch600" else "single"] * nodes,
                          "traffic_note": "bytes per launch: dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                         "ncu capture (profiles/k_step_f32_batch600_traffic.md, "
+                                         "ncu capture (profiles/k_step_f32_batch100_traffic.md, "
                                          "profiles/k_step_f32_drop4096_traffic.md), per node, times the "
                                          "nodes of one launch"},
             "fp32_single_4096": single32,

@@ -400,14 +400,17 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #ifndef ITLBM_F32_BLOCKS
 #define ITLBM_F32_BLOCKS 4
 #endif
+#ifndef ITLBM_FOLD_BLOCKS  // the fold at 5 or 6 CTAs per SM (48 or 40 registers, with spills) measured
+#define ITLBM_FOLD_BLOCKS 4   // 17 % and 8 % slower on the 600-case batch
+#endif
 #ifdef ITLBM_STEP_F64
-#define ITLBM_STEP_MIN_BLOCKS (ITLBM_F64_BLOCKS * 256 / STEP_THREADS)
+#define ITLBM_STEP_MIN_BLOCKS(fold) (ITLBM_F64_BLOCKS * 256 / STEP_THREADS)
 #else
-#define ITLBM_STEP_MIN_BLOCKS (ITLBM_F32_BLOCKS * 256 / STEP_THREADS)
+#define ITLBM_STEP_MIN_BLOCKS(fold) (((fold) ? ITLBM_FOLD_BLOCKS : ITLBM_F32_BLOCKS) * 256 / STEP_THREADS)
 #endif
 
 template <class S, bool FOLD, int W>
-__global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS) k_step(const CaseDev *__restrict__ cases,
+__global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS(FOLD)) k_step(const CaseDev *__restrict__ cases,
                                                        const TileRef *__restrict__ tiles,
                                                        int ntiles, const int *__restrict__ ntiles_dev,
                                                        int k, int aux_k) {

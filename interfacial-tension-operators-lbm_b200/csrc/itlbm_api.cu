@@ -97,10 +97,12 @@ bool narrow_edges_default() {
 void case_layout(CaseDev &h, int nx, int ny, int prec) {
     h.nx = nx;
     h.ny = ny;
-    h.pitch = (nx + 31) / 32 * 32;
-    h.stride = (long long)h.pitch * ny;
     h.tiles_x = (nx + TX - 1) / TX;
+    h.pitch = h.tiles_x * TX;
     h.tiles = h.tiles_x * ((ny + TY - 1) / TY);
+    h.tile_elems = 2 * planes_of(prec) * PLANE;
+    h.buf_elems = buf_elems_of(nx, ny, prec);
+    h.aux_stride = aux_elems_of(nx, ny);
     h.prec = prec;
 }
 
@@ -266,7 +268,7 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
     fill_params(h, d->op, d->tau, d->A_fact, d->beta, d->rho_B > 0 ? d->rho_B : 1.0);
     fill_shift(h, h.rho0, d->geometry == ITLBM_GEOM_DROP ? d->v0 : 0.0);
     const size_t elem = elem_of(d->precision);
-    const size_t per_buf = (size_t)2 * planes_of(d->precision) * h.stride * elem;
+    const size_t per_buf = (size_t)h.buf_elems * elem;
     if ((e = cudaMalloc(&c->mem, 2 * per_buf)) != cudaSuccess) {
         itlbm_case_destroy(c);
         return cuda_fail(e, "cudaMalloc(state)");
@@ -302,12 +304,12 @@ int itlbm_case_create(const itlbm_case_desc *d, itlbm_case **out) {
 
 static int ensure_aux(itlbm_case *c) {
     if (c->aux) return ITLBM_OK;
-    cudaError_t e = cudaMalloc(&c->aux, sizeof(double) * 4 * (size_t)c->host.stride);
+    cudaError_t e = cudaMalloc(&c->aux, sizeof(double) * 4 * (size_t)c->host.aux_stride);
     if (e != cudaSuccess) {
         c->aux = nullptr;
         return cuda_fail(e, "cudaMalloc(aux)");
     }
-    cudaMemset(c->aux, 0, sizeof(double) * 4 * (size_t)c->host.stride);
+    cudaMemset(c->aux, 0, sizeof(double) * 4 * (size_t)c->host.aux_stride);
     c->host.aux = c->aux;
     e = cudaMemcpy(c->dev, &c->host, sizeof(CaseDev), cudaMemcpyHostToDevice);
     // a pageable copy may return before the data lands, and the steps may go to a non-blocking stream
@@ -540,7 +542,7 @@ static int read_fields_as(itlbm_case *c, int form, double *rho_R, double *rho_B,
         std::vector<double> a(3 * n);
         for (int k = 0; k < 3 && e == cudaSuccess; k++)
             e = cudaMemcpy2D(a.data() + k * n, sizeof(double) * c->host.nx,
-                             c->aux + (size_t)k * c->host.stride, sizeof(double) * c->host.pitch,
+                             c->aux + (size_t)k * c->host.aux_stride, sizeof(double) * c->host.pitch,
                              sizeof(double) * c->host.nx, c->host.ny, cudaMemcpyDeviceToHost);
         for (size_t p = 0; p < n; p++)
             for (int k = 0; k < 3; k++) force[3 * p + k] = a[k * n + p];
@@ -641,7 +643,7 @@ int itlbm_dev_calcula_forca(const itlbm_operador *op, double sigma, int nx, int 
         std::vector<double> a(3 * n);
         cudaError_t e = cudaSuccess;
         for (int k = 0; k < 3 && e == cudaSuccess; k++)
-            e = cudaMemcpy2D(a.data() + k * n, sizeof(double) * nx, c->aux + (size_t)k * c->host.stride,
+            e = cudaMemcpy2D(a.data() + k * n, sizeof(double) * nx, c->aux + (size_t)k * c->host.aux_stride,
                              sizeof(double) * c->host.pitch, sizeof(double) * nx, ny, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) r = cuda_fail(e, "dev_calcula_forca");
         else

@@ -66,11 +66,10 @@ struct Active {
 };
 
 size_t case_bytes(const itlbm_case_desc &d, bool &need_aux) {
-    const long long pitch = (d.nx + 31) / 32 * 32;
-    const long long stride = pitch * d.ny;
     const size_t elem = elem_of(d.precision);
     need_aux = d.op.tipo >= ITLBM_OP_F1 || d.geometry == ITLBM_GEOM_STRIP;
-    return (size_t)2 * 2 * planes_of(d.precision) * stride * elem + (need_aux ? (size_t)4 * stride * 8 : 0);
+    return (size_t)2 * buf_elems_of(d.nx, d.ny, d.precision) * elem +
+           (need_aux ? (size_t)4 * aux_elems_of(d.nx, d.ny) * 8 : 0);
 }
 
 // the work tables, per storage form: [0] FP64, [1] FP32, [2] FP32 fold
@@ -475,10 +474,10 @@ int admit_cases(itlbm_batch *b) {
         fill_params(h, d.op, d.tau, d.A_fact, d.beta, d.rho_B > 0 ? d.rho_B : 1.0);
         fill_shift(h, h.rho0, d.geometry == ITLBM_GEOM_DROP ? d.v0 : 0.0);
         const size_t elem = elem_of(d.precision);
-        const size_t per_buf = (size_t)2 * planes_of(d.precision) * h.stride * elem;
+        const size_t per_buf = (size_t)h.buf_elems * elem;
         cudaError_t e = cudaMallocFromPoolAsync(&a->mem, 2 * per_buf, b->pool, b->stream);
         if (e == cudaSuccess && need_aux)
-            e = cudaMallocFromPoolAsync(&a->aux, sizeof(double) * 4 * (size_t)h.stride, b->pool, b->stream);
+            e = cudaMallocFromPoolAsync(&a->aux, sizeof(double) * 4 * (size_t)h.aux_stride, b->pool, b->stream);
         if (e != cudaSuccess) {
             if (a->mem) cudaFreeAsync(a->mem, b->stream);
             delete a;
@@ -489,7 +488,7 @@ int admit_cases(itlbm_batch *b) {
             cudaFreeAsync(a->mem, b->stream);
             if (a->aux) cudaFreeAsync(a->aux, b->stream);
             delete a;
-            return cuda_fail(e, "state tensor map");
+            return cuda_fail(e, "state buffers");
         }
         h.aux = a->aux;
         h.parity0 = 0;

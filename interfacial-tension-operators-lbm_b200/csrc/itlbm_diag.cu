@@ -43,9 +43,9 @@ __device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int 
             constexpr int i = decltype(I)::value;
             const int xs = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
             const int ys = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
-            const long long o = (long long)ys * c.pitch + xs;
-            fR[i] = d[(long long)i * c.stride + o];
-            fB[i] = d[(long long)(NV + i) * c.stride + o];
+            const long long o = node_off(c, xs, ys);
+            fR[i] = d[o + i * PLANE];
+            fB[i] = d[o + (NV + i) * PLANE];
         });
     } else if (c.prec == ITLBM_PREC_F32) {
         const float *d = (const float *)c.buf[cur];
@@ -53,9 +53,9 @@ __device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int 
             constexpr int i = decltype(I)::value;
             const int xs = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
             const int ys = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
-            const long long o = (long long)ys * c.pitch + xs;
-            const double e = d[(long long)i * c.stride + o];
-            const double dd = d[(long long)(NV + i) * c.stride + o];
+            const long long o = node_off(c, xs, ys);
+            const double e = d[o + i * PLANE];
+            const double dd = d[o + (NV + i) * PLANE];
             const double f = (double)c.sh[i] + e;
             fR[i] = 0.5 * (f + dd);
             fB[i] = 0.5 * (f - dd);
@@ -68,10 +68,10 @@ __device__ __forceinline__ void post_pops(const CaseDev &c, int cur, int x, int 
             constexpr int K = fold_class(i);
             const int xs = cx(i) == 0 ? x : (cx(i) > 0 ? xp : xm);
             const int ys = cy(i) == 0 ? y : (cy(i) > 0 ? yp : ym);
-            const long long o = (long long)ys * c.pitch + xs;
+            const long long o = node_off(c, xs, ys);
             const double share = wgt<double>(i) / wk<double>(K);
-            const double f = ((double)c.shk[K] + d[(long long)K * c.stride + o]) * share;
-            const double dd = d[(long long)(NK + K) * c.stride + o] * share;
+            const double f = ((double)c.shk[K] + d[o + K * PLANE]) * share;
+            const double dd = d[o + (NK + K) * PLANE] * share;
             fR[i] = 0.5 * (f + dd);
             fB[i] = 0.5 * (f - dd);
         });
@@ -229,10 +229,10 @@ __global__ void __launch_bounds__(DT) k_drop_d1(const DiagJob *__restrict__ jobs
         }
         double F0 = 0, F1 = 0, F2 = 0;
         if (ok && use_force) {
-            const long long o = (long long)y * c.pitch + x;
+            const long long o = aux_off(c, x, y);
             F0 = c.aux[o];
-            F1 = c.aux[c.stride + o];
-            F2 = c.aux[2 * c.stride + o];
+            F1 = c.aux[c.aux_stride + o];
+            F2 = c.aux[2 * c.aux_stride + o];
             if (!finite_d(F0) || !finite_d(F1) || !finite_d(F2)) {
                 ++bad;
                 ok = false;
@@ -301,8 +301,8 @@ __global__ void __launch_bounds__(DT) k_drop_d1(const DiagJob *__restrict__ jobs
         double uyd = (rho_R * vyR + rho_B * vyB) / rh;
         double uzd = (rho_R * vzR + rho_B * vzB) / rh;
         if (use_force) {
-            const long long o = (long long)y * c.pitch + x;
-            const double G0 = c.aux[o], G1 = c.aux[c.stride + o], G2 = c.aux[2 * c.stride + o];
+            const long long o = aux_off(c, x, y);
+            const double G0 = c.aux[o], G1 = c.aux[c.aux_stride + o], G2 = c.aux[2 * c.aux_stride + o];
             uxd = uxd - 0.5 * G0 / rh;
             uyd = uyd - 0.5 * G1 / rh;
             uzd = uzd - 0.5 * G2 / rh;
@@ -803,9 +803,9 @@ __global__ void __launch_bounds__(DT) k_strip_s1(const DiagJob *__restrict__ job
             v[S_RUIM] += 1.0;
             continue;
         }
-        const long long o = (long long)y * c.pitch + x;
+        const long long o = aux_off(c, x, y);
         if (use_force) {
-            const double F0 = c.aux[o], F1 = c.aux[c.stride + o];
+            const double F0 = c.aux[o], F1 = c.aux[c.aux_stride + o];
             jx -= 0.5 * F0;
             jy -= 0.5 * F1;
             v[S_SFX] += F0;
@@ -824,7 +824,7 @@ __global__ void __launch_bounds__(DT) k_strip_s1(const DiagJob *__restrict__ job
         const double Pnn = nx_ * nx_ * Pxx + 2 * nx_ * ny_ * Pxy + ny_ * ny_ * Pyy;
         const double Ptt = tx_ * tx_ * Pxx + 2 * tx_ * ty_ * Pxy + ty_ * ty_ * Pyy;
         v[S_SIGPOP] += Pnn - 0.5 * (Ptt + Pzz);
-        v[S_INTGRAD] += c.aux[3 * c.stride + o];
+        v[S_INTGRAD] += c.aux[3 * c.aux_stride + o];
         const double dd = dist_central(x, y, p, q, N);
         const double cR = rR / rho;
         if (cR > 0.02 && cR < 0.98 && fabs(dd) < 8.0) {
@@ -977,7 +977,7 @@ __global__ void k_fields(const CaseDev *__restrict__ cp, int cur, int use_force,
         for (int i = 0; i < NV; i++) rr = __dadd_rn(rr, fR[i]);
 #pragma unroll
         for (int i = 0; i < NV; i++) rb = __dadd_rn(rb, fB[i]);
-        const long long o = (long long)y * c.pitch + x;
+        const long long o = aux_off(c, x, y);
         double vx, vy, vz;
         if (form == ITLBM_FIELDS_VTK) {
             double m[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
@@ -1014,8 +1014,8 @@ __global__ void k_fields(const CaseDev *__restrict__ cp, int cur, int use_force,
             const double rho = __dadd_rn(rr, rb);
             if (use_force && rho > 0.0) {
                 vx = __dsub_rn(vx, __dmul_rn(0.5, c.aux[o]) / rho);
-                vy = __dsub_rn(vy, __dmul_rn(0.5, c.aux[c.stride + o]) / rho);
-                vz = __dsub_rn(vz, __dmul_rn(0.5, c.aux[2 * c.stride + o]) / rho);
+                vy = __dsub_rn(vy, __dmul_rn(0.5, c.aux[c.aux_stride + o]) / rho);
+                vz = __dsub_rn(vz, __dmul_rn(0.5, c.aux[2 * c.aux_stride + o]) / rho);
             }
         } else {
             double jx = 0.0, jy = 0.0, jz = 0.0;
@@ -1032,8 +1032,8 @@ __global__ void k_fields(const CaseDev *__restrict__ cp, int cur, int use_force,
             } else {
                 if (use_force) {
                     jx = __dsub_rn(jx, __dmul_rn(0.5, c.aux[o]));
-                    jy = __dsub_rn(jy, __dmul_rn(0.5, c.aux[c.stride + o]));
-                    jz = __dsub_rn(jz, __dmul_rn(0.5, c.aux[2 * c.stride + o]));
+                    jy = __dsub_rn(jy, __dmul_rn(0.5, c.aux[c.aux_stride + o]));
+                    jz = __dsub_rn(jz, __dmul_rn(0.5, c.aux[2 * c.aux_stride + o]));
                 }
                 vx = jx / rho;
                 vy = jy / rho;

@@ -26,14 +26,14 @@ __device__ void store_state(const CaseDev &c, int buf, long long off, const doub
     if (c.prec == ITLBM_PREC_F64) {
         double *d = (double *)c.buf[buf];
         for (int i = 0; i < NV; i++) {
-            d[(long long)i * c.stride + off] = fR[i];
-            d[(long long)(NV + i) * c.stride + off] = fB[i];
+            d[off + i * PLANE] = fR[i];
+            d[off + (NV + i) * PLANE] = fB[i];
         }
     } else if (c.prec == ITLBM_PREC_F32) {
         float *d = (float *)c.buf[buf];
         for (int i = 0; i < NV; i++) {
-            d[(long long)i * c.stride + off] = (float)((fR[i] + fB[i]) - (double)c.sh[i]);
-            d[(long long)(NV + i) * c.stride + off] = (float)(fR[i] - fB[i]);
+            d[off + i * PLANE] = (float)((fR[i] + fB[i]) - (double)c.sh[i]);
+            d[off + (NV + i) * PLANE] = (float)(fR[i] - fB[i]);
         }
     } else {  // fold: class sums of the members (FP64), then shifted and rounded
         float *d = (float *)c.buf[buf];
@@ -43,8 +43,8 @@ __device__ void store_state(const CaseDev &c, int buf, long long off, const doub
             Dk[fold_class(i)] += fR[i] - fB[i];
         }
         for (int K = 0; K < NK; K++) {
-            d[(long long)K * c.stride + off] = (float)(F[K] - (double)c.shk[K]);
-            d[(long long)(NK + K) * c.stride + off] = (float)Dk[K];
+            d[off + K * PLANE] = (float)(F[K] - (double)c.shk[K]);
+            d[off + (NK + K) * PLANE] = (float)Dk[K];
         }
     }
 }
@@ -113,7 +113,7 @@ __global__ void k_init(const CaseDev *__restrict__ cp, int geometry, const doubl
                 fB[i] = wgt<double>(i) * (1.0 - cR);
             }
         }
-        store_state(c, c.parity0, (long long)y * c.pitch + x, fR, fB);
+        store_state(c, c.parity0, node_off(c, x, y), fR, fB);
     }
 }
 
@@ -139,23 +139,23 @@ __global__ void k_export(const CaseDev *__restrict__ cp, int cur, int which, dou
                     xs = wrapi(x + kx(K), c.nx);
                     ys = wrapi(y + ky(K), c.ny);
                 }
-                const long long off = (long long)ys * c.pitch + xs;
+                const long long off = node_off(c, xs, ys);
                 const float *d = (const float *)c.buf[cur];
-                unfold_split(d[(long long)K * c.stride + off], d[(long long)(NK + K) * c.stride + off], K, i,
+                unfold_split(d[off + K * PLANE], d[off + (NK + K) * PLANE], K, i,
                              (double)c.shk[K], r, b);
                 oR[t * NV + i] = r;
                 oB[t * NV + i] = b;
                 continue;
             }
-            const long long off = (long long)ys * c.pitch + xs;
+            const long long off = node_off(c, xs, ys);
             if (c.prec == ITLBM_PREC_F64) {
                 const double *d = (const double *)c.buf[cur];
-                r = d[(long long)i * c.stride + off];
-                b = d[(long long)(NV + i) * c.stride + off];
+                r = d[off + i * PLANE];
+                b = d[off + (NV + i) * PLANE];
             } else {
                 const float *d = (const float *)c.buf[cur];
-                const double e = d[(long long)i * c.stride + off];
-                const double dd = d[(long long)(NV + i) * c.stride + off];
+                const double e = d[off + i * PLANE];
+                const double dd = d[off + (NV + i) * PLANE];
                 const double f = (double)c.sh[i] + e;
                 r = 0.5 * (f + dd);
                 b = 0.5 * (f - dd);
@@ -173,7 +173,7 @@ __global__ void k_import(const CaseDev *__restrict__ cp, int cur, const double *
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(t % c.nx), y = (int)(t / c.nx);
-        store_state(c, cur, (long long)y * c.pitch + x, iR + t * NV, iB + t * NV);
+        store_state(c, cur, node_off(c, x, y), iR + t * NV, iB + t * NV);
     }
 }
 

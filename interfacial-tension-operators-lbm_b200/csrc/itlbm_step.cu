@@ -1,7 +1,8 @@
 // itlbm_step.cu -- the fused time step, the initial state and population export/import.
 //
-// State layout in HBM (per case, per buffer): 2 colours x 19 directions x `stride` elements, one
-// structure-of-arrays plane per (colour, i), rows of `pitch` elements (pitch = nx rounded up to 32).
+// State layout in HBM (per case, per buffer): tile-major (CaseDev in itlbm_internal.h).  Each 32 x 8
+// tile is one contiguous block of 2 colours x 19 directions planes of 256 nodes, so every plane of a
+// node is at a compile-time offset (q x 256 elements) from the node's address.
 //   FP64 plain:  plane (0, i) = f_R,i and (1, i) = f_B,i
 //   FP32 shifted: plane (0, i) = e_i = f_i - w_i rho0 and (1, i) = d_i = f_R,i - f_B,i
 // A buffer holds the populations at the top of a step -- the reference's inif_R / inif_B after the
@@ -151,11 +152,10 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     constexpr int QX = SmemT<S, W, Hh>::QX, QY = SmemT<S, W, Hh>::QY;
     const int tid = threadIdx.x;
     const int lx = tid % W, ly = tid / W;
-    const int nx = c.nx, ny = c.ny, pitch = c.pitch;
-    const long long stride = c.stride;
-    // plane q of a buffer (uniform across the CTA); offsets within a plane are 32-bit (a plane holds
-    // fewer than 2^31 elements: boxes are capped at 2^30 nodes and 65535 tile rows)
-    auto plane = [stride](auto *buf, int q) { return buf + (long long)q * stride; };
+    const int nx = c.nx, ny = c.ny, tiles_x = c.tiles_x;
+    constexpr int TE = 2 * NP * PLANE;  // elements per tile block
+    // the address of node (x, y) in a buffer; plane q of the node is at [q * PLANE] from it
+    auto node = [tiles_x](auto *buf, int x_, int y_) { return buf + node_off(tiles_x, TE, x_, y_); };
     const int x0 = (int)((unsigned)tile & 0xFFFFu) * 8, y0 = (int)((unsigned)tile >> 16) * 8;
     const int xe = min(x0 + W, nx), ye = min(y0 + Hh, ny);  // end of the valid interior
     const int H = c.halo;
@@ -171,12 +171,12 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     double sbd = 0.0;
     if (x < xe + H && y < ye + H) {
         const int xw = valid ? x : wrap_near(x, nx), yw = valid ? y : wrap_near(y, ny);
-        const int off = yw * pitch + xw;
+        const S *own = node(src, xw, yw);
         S a[NP], b[NP];
 #pragma unroll
-        for (int i = 0; i < NP; i++) a[i] = ldg<LD_OWN>(plane(src, i) + off);
+        for (int i = 0; i < NP; i++) a[i] = ldg<LD_OWN>(own + i * PLANE);
 #pragma unroll
-        for (int i = 0; i < NP; i++) b[i] = ldg<LD_OWN>(plane(src, NP + i) + off);
+        for (int i = 0; i < NP; i++) b[i] = ldg<LD_OWN>(own + (NP + i) * PLANE);
 #pragma unroll
         for (int i = 0; i < NP; i++) sa = sa + a[i];
 #pragma unroll
@@ -203,10 +203,10 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         ring_pos<W, Hh>(r, H, px, py);
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
         if (gx < xe + H && gy < ye + H) {
-            const int off = wrap_near(gy, ny) * pitch + wrap_near(gx, nx);
+            const S *rn = node(src, wrap_near(gx, nx), wrap_near(gy, ny)) + colour * NP * PLANE;
             S v[NP];
 #pragma unroll
-            for (int i = 0; i < NP; i++) v[i] = ldg<LD_RING>(plane(src, colour * NP + i) + off);
+            for (int i = 0; i < NP; i++) v[i] = ldg<LD_RING>(rn + i * PLANE);
             S acc = S(0);
 #pragma unroll
             for (int i = 0; i < NP; i++) acc = acc + v[i];
@@ -293,13 +293,12 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             Fy = mu * g1;
             Fz = mu * g2;
         }
+        // the destination node x + c_i (periodic) of D3Q19 direction i, or of class i of the fold
         const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
         const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
-        auto dst_off = [&](int i) {  // D3Q19 direction i, or class i of the fold
+        auto dst_node = [&](int i) {
             const int ex = FOLD ? kx(i) : cx(i), ey = FOLD ? ky(i) : cy(i);
-            const int xd = ex == 0 ? x : (ex > 0 ? xp : xm);
-            const int yd = ey == 0 ? y : (ey > 0 ? yp : ym);
-            return yd * pitch + xd;
+            return node(dst, ex == 0 ? x : (ex > 0 ? xp : xm), ey == 0 ? y : (ey > 0 ? yp : ym));
         };
         bool skip;
         if constexpr (FOLD) {
@@ -316,15 +315,15 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                                        shift_of<kx(K + 1)>(c, wk<float>(K + 1)), dK, dJ);
                     dsum += (double)dK;
                     dsum += (double)dJ;
-                    const int oK = dst_off(K), oJ = dst_off(K + 1);
-                    stg(plane(dst, K) + oK, f[K]);
-                    stg(plane(dst, NK + K) + oK, dK);
-                    stg(plane(dst, K + 1) + oJ, f[K + 1]);
-                    stg(plane(dst, NK + K + 1) + oJ, dJ);
+                    float *nK = dst_node(K), *nJ = dst_node(K + 1);
+                    stg(nK + K * PLANE, f[K]);
+                    stg(nK + (NK + K) * PLANE, dK);
+                    stg(nJ + (K + 1) * PLANE, f[K + 1]);
+                    stg(nJ + (NK + K + 1) * PLANE, dJ);
                 });
-                const int o0 = dst_off(0);
-                stg(dst + o0, f[0]);
-                stg(plane(dst, NK) + o0, (float)(sbd - dsum));
+                float *n0 = dst_node(0);
+                stg(n0, f[0]);
+                stg(n0 + NK * PLANE, (float)(sbd - dsum));
             }
         } else if constexpr (std::is_same<S, double>::value) {
             Recolour64 rc;
@@ -336,9 +335,9 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                     constexpr int i = decltype(I)::value;
                     double r, b;
                     split64<i>(rc, f[i], r, b);
-                    const int o = dst_off(i);
-                    stg(plane(dst, i) + o, r);
-                    stg(plane(dst, NV + i) + o, b);
+                    double *n = dst_node(i);
+                    stg(n + i * PLANE, r);
+                    stg(n + (NV + i) * PLANE, b);
                 });
             }
         } else {
@@ -359,30 +358,30 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                                     shift_of<cx(i + 1)>(c, wgt<float>(i + 1)), di, dj);
                     dsum += (double)di;
                     dsum += (double)dj;
-                    const int oi = dst_off(i), oj = dst_off(i + 1);
-                    stg(plane(dst, i) + oi, f[i]);
-                    stg(plane(dst, NV + i) + oi, di);
-                    stg(plane(dst, i + 1) + oj, f[i + 1]);
-                    stg(plane(dst, NV + i + 1) + oj, dj);
+                    float *ni = dst_node(i), *nj = dst_node(i + 1);
+                    stg(ni + i * PLANE, f[i]);
+                    stg(ni + (NV + i) * PLANE, di);
+                    stg(nj + (i + 1) * PLANE, f[i + 1]);
+                    stg(nj + (NV + i + 1) * PLANE, dj);
                 });
-                const int o0 = dst_off(0);
-                stg(dst + o0, f[0]);
-                stg(plane(dst, NV) + o0, (float)(sbd - dsum));
+                float *n0 = dst_node(0);
+                stg(n0, f[0]);
+                stg(n0 + NV * PLANE, (float)(sbd - dsum));
             }
         }
         if (skip) {  // rho <= 1e-30: the site is streamed unchanged (Operadores_tensao.cpp:347)
-            const int off = y * pitch + x;
+            const S *own = node(src, x, y);
             sfor<0, NP>([&](auto I) {
                 constexpr int i = decltype(I)::value;
-                const int o = dst_off(i);
-                plane(dst, i)[o] = plane(src, i)[off];
-                plane(dst, NP + i)[o] = plane(src, NP + i)[off];
+                S *n = dst_node(i);
+                n[i * PLANE] = own[i * PLANE];
+                n[(NP + i) * PLANE] = own[(NP + i) * PLANE];
             });
         }
 
         if (c.aux != nullptr && (k == aux_k || (c.aux_at_end && k == c.chunk_len - 1))) {
-            const long long o = (long long)y * pitch + x;
-            const long long n = stride;
+            const long long o = aux_off(c, x, y);
+            const long long n = c.aux_stride;
             c.aux[o] = (double)Fx;
             c.aux[n + o] = (double)Fy;
             c.aux[2 * n + o] = (double)Fz;

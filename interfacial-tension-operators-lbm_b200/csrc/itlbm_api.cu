@@ -60,6 +60,16 @@ void fill_params(CaseDev &c, const itlbm_operador &op, double tau, double A_fact
     }
     c.kf = 0.75 * A_fact * op.xi;           // Operadores_tensao.cpp:240
     c.bf = 3.0 * A_fact / (8.0 * op.xi);    // Operadores_tensao.cpp:241
+    c.pf.inv_tau = (float)c.inv_tau;
+    c.pf.fac3 = 3.0f * (float)c.src_factor;
+    c.pf.A = (float)c.A;
+    c.pf.B1 = (float)c.B1;
+    c.pf.B2 = (float)c.B2;
+    c.pf.Bax = (float)(c.B1 + 2.0 * c.B2);
+    c.pf.beta = (float)c.beta;
+    c.pf.sigma = (float)c.sigma;
+    c.pf.kf = (float)c.kf;
+    c.pf.bf = (float)c.bf;
     fill_shift(c, rho0, 0.0);
 }
 
@@ -68,13 +78,15 @@ void fill_shift(CaseDev &c, double rho0, double u0x) {
     c.rho0 = rho0;
     c.u0x = u0x;
     const double u2 = u0x * u0x;
-    c.j0x = (float)(rho0 * u0x);
-    c.u0b = (float)(rho0 * u2);
-    c.s0 = (float)(rho0 * (1.0 - 1.5 * u2));
-    c.sx = (float)(rho0 * (1.0 + 3.0 * u2));  // s0 + 4.5 rho0 u0x^2
-    c.j3 = (float)(3.0 * rho0 * u0x);
+    CaseDev::F32Par &p = c.pf;
+    p.rho0 = (float)rho0;
+    p.j0x = (float)(rho0 * u0x);
+    p.u0b = (float)(rho0 * u2);
+    p.s0 = (float)(rho0 * (1.0 - 1.5 * u2));
+    p.sx = (float)(rho0 * (1.0 + 3.0 * u2));  // s0 + 4.5 rho0 u0x^2
+    p.j3 = (float)(3.0 * rho0 * u0x);
     // the float operations of shift_of (itlbm_site.cuh), so that host and device agree to the bit
-    auto shift = [&](float w, int ex) { return w * (ex == 0 ? c.s0 : (ex > 0 ? c.sx + c.j3 : c.sx - c.j3)); };
+    auto shift = [&](float w, int ex) { return w * (ex == 0 ? p.s0 : (ex > 0 ? p.sx + p.j3 : p.sx - p.j3)); };
     for (int i = 0; i < NV; i++) c.sh[i] = shift(wgt<float>(i), cx(i));
     for (int K = 0; K < NK; K++) c.shk[K] = shift(wk<float>(K), kx(K));
 }

@@ -132,14 +132,25 @@ struct CaseDev {
     // form s_i = w_i (c_ix == 0 ? s0 : sx +- j3) from three floats; sh and shk hold the same values,
     // formed by the host with the same float operations, for import, export and the diagnostics.
     double u0x;
-    float j0x;             // rho0 u0x
-    float u0b;             // rho0 u0x^2
-    float s0;              // rho0 (1 - 1.5 u0x^2): s_i / w_i of the directions with c_ix = 0
-    float sx;              // s0 + 4.5 rho0 u0x^2
-    float j3;              // 3 rho0 u0x
     float sh[NV];          // s_i of each direction
     float shk[NK];         // fold: shift of each class, the sum of its members' s_i
+    // The parameters of the FP32 kernels, rounded to float once by the host (the same roundings the
+    // kernels made per thread before), in one 16-byte aligned block read with four vector loads.
+    struct alignas(16) F32Par {
+        float rho0, inv_tau, fac3, A;  // fac3 = 3 src_factor
+        float B1, B2, Bax, beta;       // Bax = B1 + 2 B2 (the fold's axis classes)
+        float sigma, kf, bf, j0x;      // j0x = rho0 u0x
+        float u0b, s0, sx, j3;         // rho0 u0x^2; rho0 (1 - 1.5 u0x^2), the s_i / w_i of the
+                                       // directions with c_ix = 0; s0 + 4.5 rho0 u0x^2; 3 rho0 u0x
+    } pf;
 };
+
+// The FP32 parameter block of a case, four 16-byte loads.
+__device__ __forceinline__ CaseDev::F32Par load_pf(const CaseDev &c) {
+    const float4 *q = reinterpret_cast<const float4 *>(&c.pf);
+    const float4 a = q[0], b = q[1], d = q[2], e = q[3];
+    return CaseDev::F32Par{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, d.x, d.y, d.z, d.w, e.x, e.y, e.z, e.w};
+}
 
 // Offset of node (x, y) within a state buffer (tile-major, see CaseDev; plane q adds q * PLANE),
 // and within an auxiliary array (plain rows).  Tile indices fit 32 bits (each side of a box is at

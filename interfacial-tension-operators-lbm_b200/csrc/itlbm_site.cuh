@@ -231,10 +231,10 @@ __device__ __forceinline__ void colisao_site_f64(double (&fR)[NV], double (&fB)[
 // The shift s of a direction (or class) with x velocity ex: w (s0 + 3 c.J0 + 4.5 (c.J0)(c.U0)), the
 // equilibrium at rho0 and U0 = (u0x, 0) (CaseDev).
 template <int ex>
-__device__ __forceinline__ float shift_of(const CaseDev &c, float w) {
-    if constexpr (ex == 0) return w * c.s0;
-    else if constexpr (ex > 0) return w * (c.sx + c.j3);
-    else return w * (c.sx - c.j3);
+__device__ __forceinline__ float shift_of(const CaseDev::F32Par &p, float w) {
+    if constexpr (ex == 0) return w * p.s0;
+    else if constexpr (ex > 0) return w * (p.sx + p.j3);
+    else return w * (p.sx - p.j3);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -286,8 +286,8 @@ __device__ __forceinline__ void split32_pair(const Recolour32 &r, float ei, floa
 template <bool FORCE>
 __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D, float gmx,
                                             float gmy, float gmz, float Fx, float Fy, float Fz,
-                                            const CaseDev &c, Recolour32 &rc) {
-    const float rho0 = (float)c.rho0;
+                                            const CaseDev::F32Par &p, Recolour32 &rc) {
+    const float rho0 = p.rho0;
     const float rho = rho0 + drho;
     rc.skip = !(rho > 1.0e-30f);
     if (rc.skip) return;
@@ -313,13 +313,13 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
     // Delta = sum c_i e_i + F / 2 and the velocity u* = (rho0 U0 + Delta) / rho
     const float Dx = FORCE ? fmaf(0.5f, Fx, jx) : jx, Dy = FORCE ? fmaf(0.5f, Fy, jy) : jy;
     const float Dz = FORCE ? fmaf(0.5f, Fz, jz) : jz;
-    const float vx = (c.j0x + Dx) * inv_rho, vy = Dy * inv_rho, vz = Dz * inv_rho;
+    const float vx = (p.j0x + Dx) * inv_rho, vy = Dy * inv_rho, vz = Dz * inv_rho;
     const float s15 = 1.5f * inv_rho, s45 = 4.5f * inv_rho;
-    const float usq15 = s15 * (fmaf(Dx, fmaf(2.0f, c.j0x, Dx), fmaf(Dy, Dy, Dz * Dz)) - drho * c.u0b);
-    const float inv_tau = (float)c.inv_tau;
+    const float usq15 = s15 * (fmaf(Dx, fmaf(2.0f, p.j0x, Dx), fmaf(Dy, Dy, Dz * Dz)) - drho * p.u0b);
+    const float inv_tau = p.inv_tau;
     const float Frx = ax * rho, Fry = ay * rho, Frz = az * rho;
     const float vF = Frx * vx + Fry * vy + Frz * vz;
-    const float fac3 = 3.0f * (float)c.src_factor;
+    const float fac3 = p.fac3;
     // BGK (+ Guo source) of the moving populations, pair (i, j) with c_j = -c_i, d = c_i.Delta:
     //   f_eq - s = w (drho + 4.5 (d (a + d) - drho b) / rho - usq15 +- 3 d),  a = 2 rho0 c.U0, b = rho0 (c.U0)^2
     //   S = 3 (1 - 1/2tau) w (3 (c.F)(c.u) - u.F +- c.F)
@@ -329,7 +329,7 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
         const float cD = cdotp<i>(Dx, Dy, Dz);
         float q;  // (c.Delta) (2 rho0 c.U0 + c.Delta) - drho rho0 (c.U0)^2
         if constexpr (cx(i) == 0) q = cD * cD;
-        else q = fmaf(cD, fmaf(cx(i) > 0 ? 2.0f : -2.0f, c.j0x, cD), -drho * c.u0b);
+        else q = fmaf(cD, fmaf(cx(i) > 0 ? 2.0f : -2.0f, p.j0x, cD), -drho * p.u0b);
         const float sym = w * fmaf(s45, q, drho - usq15);
         const float asym = (3.0f * w) * cD;
         float ei = fmaf((sym + asym) - e[i], inv_tau, e[i]);
@@ -348,11 +348,11 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
     const float mod = sqrtf(mod2);
     if constexpr (!FORCE) {
         // class P: f_i += A |g| (w_i (c_i.g)^2 / |g|^2 - B_i), the same for both of a pair
-        const float A = (float)c.A;
+        const float A = p.A;
         if (!(mod2 <= 1.0e-30f || A == 0.0f)) {
             const float inv2 = 1.0f / mod2;
             const float amod = A * mod;
-            const float B1 = (float)c.B1, B2 = (float)c.B2;
+            const float B1 = p.B1, B2 = p.B2;
             sfor<0, 9>([&](auto M) {
                 constexpr int i = 2 * decltype(M)::value + 1;
                 constexpr float w = wgt<float>(i);
@@ -371,7 +371,7 @@ __device__ __forceinline__ void collide_f32(float (&e)[NV], float drho, float D,
         float s2 = (e[9] + e[10]) + (e[11] + e[12]), s3 = (e[13] + e[14]) + (e[15] + e[16]);
         e[0] = drho - (((s0 + s1) + (s2 + s3)) + (e[17] + e[18]));
     }
-    const float fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
+    const float fat2 = 0.5f * p.beta * (1.0f - phi * phi) * rho;
     const float inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
     rc.phi = phi;
     rc.k1 = fat2 * wgt<float>(1) * inv_mod;
@@ -418,8 +418,8 @@ __device__ __forceinline__ void split_fold_pair(const RecolourFold &r, float eK,
 // drho = sum e_K, D = sum d_K.  The equilibrium is formed from the deviations as in collide_f32.
 template <bool FORCE>
 __device__ __forceinline__ void collide_fold(float (&e)[NK], float drho, float D, float gmx, float gmy,
-                                             float Fx, float Fy, const CaseDev &c, RecolourFold &rc) {
-    const float rho0 = (float)c.rho0;
+                                             float Fx, float Fy, const CaseDev::F32Par &p, RecolourFold &rc) {
+    const float rho0 = p.rho0;
     const float rho = rho0 + drho;
     rc.skip = !(rho > 1.0e-30f);
     if (rc.skip) return;
@@ -440,20 +440,20 @@ __device__ __forceinline__ void collide_fold(float (&e)[NK], float drho, float D
         if constexpr (ky(K) == -1) jy -= p;
     });
     const float Dx = FORCE ? fmaf(0.5f, Fx, jx) : jx, Dy = FORCE ? fmaf(0.5f, Fy, jy) : jy;
-    const float vx = (c.j0x + Dx) * inv_rho, vy = Dy * inv_rho;
+    const float vx = (p.j0x + Dx) * inv_rho, vy = Dy * inv_rho;
     const float s15 = 1.5f * inv_rho, s45 = 4.5f * inv_rho;
-    const float usq15 = s15 * (fmaf(Dx, fmaf(2.0f, c.j0x, Dx), Dy * Dy) - drho * c.u0b);
-    const float inv_tau = (float)c.inv_tau;
+    const float usq15 = s15 * (fmaf(Dx, fmaf(2.0f, p.j0x, Dx), Dy * Dy) - drho * p.u0b);
+    const float inv_tau = p.inv_tau;
     const float Frx = ax * rho, Fry = ay * rho;
     const float vF = Frx * vx + Fry * vy;
-    const float fac3 = 3.0f * (float)c.src_factor;
+    const float fac3 = p.fac3;
     sfor<0, 4>([&](auto M) {
         constexpr int K = 2 * decltype(M)::value + 1;
         constexpr float W = wk<float>(K);
         const float cD = kdot<K>(Dx, Dy);
         float q;
         if constexpr (kx(K) == 0) q = cD * cD;
-        else q = fmaf(cD, fmaf(kx(K) > 0 ? 2.0f : -2.0f, c.j0x, cD), -drho * c.u0b);
+        else q = fmaf(cD, fmaf(kx(K) > 0 ? 2.0f : -2.0f, p.j0x, cD), -drho * p.u0b);
         const float sym = W * fmaf(s45, q, drho - usq15);
         const float asym = (3.0f * W) * cD;
         float eK = fmaf((sym + asym) - e[K], inv_tau, e[K]);
@@ -471,11 +471,11 @@ __device__ __forceinline__ void collide_fold(float (&e)[NK], float drho, float D
     const float mod2 = gmx * gmx + gmy * gmy;
     const float mod = sqrtf(mod2);
     if constexpr (!FORCE) {
-        const float A = (float)c.A;
+        const float A = p.A;
         if (!(mod2 <= 1.0e-30f || A == 0.0f)) {
             const float inv2 = 1.0f / mod2;
             const float amod = A * mod;
-            const float Bax = (float)(c.B1 + 2.0 * c.B2), Bdg = (float)c.B2;
+            const float Bax = p.Bax, Bdg = p.B2;
             sfor<0, 4>([&](auto M) {
                 constexpr int K = 2 * decltype(M)::value + 1;
                 constexpr float W = wk<float>(K);
@@ -487,7 +487,7 @@ __device__ __forceinline__ void collide_fold(float (&e)[NK], float drho, float D
         }
     }
     e[0] = drho - (((e[1] + e[2]) + (e[3] + e[4])) + ((e[5] + e[6]) + (e[7] + e[8])));
-    const float fat2 = 0.5f * (float)c.beta * (1.0f - phi * phi) * rho;
+    const float fat2 = 0.5f * p.beta * (1.0f - phi * phi) * rho;
     const float inv_mod = mod > 0.0f ? 1.0f / mod : 0.0f;
     rc.phi = phi;
     rc.k1 = fat2 * ((1.0f + 0.70710678118654752f) / 18.0f) * inv_mod;

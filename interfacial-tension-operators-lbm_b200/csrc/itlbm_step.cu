@@ -96,18 +96,17 @@ struct SmemT {
     static constexpr int PX = W + 2 * HMAX, PY = Hh + 2 * HMAX;  // staged phase tile
     static constexpr int QX = W + 2, QY = Hh + 2;                // ring-1 region of the F1/F2 auxiliaries
     S phi[PY][PX];        // rho^N of tile + halo (HMAX), position (px, py) = global (x0-2+px, y0-2+py)
-    S rsum[2][PY * PX - W * Hh];  // halo ring: the two colour sums of each ring node
     S g[QY][QX][3];       // ring-1 gradient (F1, F2)
     S aux[QY][QX][AUXS];  // ring-1 normal (F1) or stress (F2), 6 values at an odd stride
 };
 
 // rho^N from the two colour sums.  FP64: (rho_R - rho_B) / (rho_R + rho_B), Imm_OPS.cpp:255-258.
 // FP32: the sums are sum e_i (rho - rho0) and sum d_i (rho_R - rho_B).
-__device__ __forceinline__ double phase_of(double rR, double rB, const CaseDev &) {
+__device__ __forceinline__ double phase_of(double rR, double rB, float) {
     return (rR - rB) / (rR + rB);
 }
-__device__ __forceinline__ float phase_of(float drho, float D, const CaseDev &c) {
-    return D / ((float)c.rho0 + drho);
+__device__ __forceinline__ float phase_of(float drho, float D, float rho0) {
+    return D / (rho0 + drho);
 }
 
 // ring position r -> staged-tile coordinates (px, py) for a halo of H (1 or 2) around the W x Hh
@@ -140,8 +139,7 @@ __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
 //   phase A  each thread loads its node: FP64 keeps f_i = f_R,i + f_B,i and the colour sums (all
 //            colisao_comum needs, Operadores_tensao.cpp:343-360), FP32 keeps e_i and the sums;
 //            the halo ring is loaded as (ring node, colour) items spread over all threads, each an
-//            ordered sum of 19 values;
-//   phase A2 rho^N of the ring from the sums;
+//            ordered sum of 19 values, and the two colours' lanes form the ring node's rho^N;
 //   phase B  F1 / F2: gradient and normal or stress on the ring-1 region;
 //   phase C  mediator gradient, force, collision, recolouring, push to x + c_i.
 // FOLD (FP32 only): the nine in-plane classes per colour instead of the 19 populations.
@@ -163,6 +161,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     const S *__restrict__ src = (const S *)c.buf[cur];
     S *__restrict__ dst = (S *)c.buf[cur ^ 1];
     const int tipo = c.tipo;
+    const float rho0f = c.pf.rho0;  // FP32: the reference density in float (phase_of)
 
     // ---- phase A ----------------------------------------------------------------------------
     const int x = x0 + lx, y = y0 + ly;
@@ -194,31 +193,29 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 #pragma unroll
             for (int i = 0; i < NP; i++) f[i] = a[i];
         }
-        sm.phi[ly + HMAX][lx + HMAX] = phase_of(sa, sb, c);
+        sm.phi[ly + HMAX][lx + HMAX] = phase_of(sa, sb, rho0f);
     }
+    // halo ring: item it = (ring node it / 2, colour it % 2), the two colours of a node on adjacent
+    // lanes, which exchange their sums by a shuffle; the loop runs in whole warps (the bound is a
+    // multiple of 32) so that every lane of a warp takes part in the shuffle
     const int nring = (W + 2 * H) * (Hh + 2 * H) - W * Hh;
-    for (int it = tid; it < 2 * nring; it += STEP_THREADS) {
-        const int colour = it >= nring ? 1 : 0, r = it - colour * nring;
-        int px, py;
-        ring_pos<W, Hh>(r, H, px, py);
+    for (int it = tid; it < ((2 * nring + 31) & ~31); it += STEP_THREADS) {
+        const int colour = it & 1, r = it >> 1;
+        int px = 0, py = 0;
+        if (r < nring) ring_pos<W, Hh>(r, H, px, py);
         const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
-        if (gx < xe + H && gy < ye + H) {
+        const bool act = r < nring && gx < xe + H && gy < ye + H;
+        S acc = S(0);
+        if (act) {
             const S *rn = node(src, wrap_near(gx, nx), wrap_near(gy, ny)) + colour * NP * PLANE;
             S v[NP];
 #pragma unroll
             for (int i = 0; i < NP; i++) v[i] = ldg<LD_RING>(rn + i * PLANE);
-            S acc = S(0);
 #pragma unroll
             for (int i = 0; i < NP; i++) acc = acc + v[i];
-            sm.rsum[colour][r] = acc;
         }
-    }
-    __syncthreads();
-    for (int r = tid; r < nring; r += STEP_THREADS) {
-        int px, py;
-        ring_pos<W, Hh>(r, H, px, py);
-        const int gx = x0 - HMAX + px, gy = y0 - HMAX + py;
-        if (gx < xe + H && gy < ye + H) sm.phi[py][px] = phase_of(sm.rsum[0][r], sm.rsum[1][r], c);
+        const S other = __shfl_xor_sync(0xffffffffu, acc, 1);
+        if (act && colour == 0) sm.phi[py][px] = phase_of(acc, other, rho0f);
     }
     __syncthreads();
 
@@ -237,7 +234,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                     g1 = -g1;
                     g2 = 0.f;
                     if (tipo == ITLBM_OP_F1) aux_normal_plane(g0, g1, sm.aux[qy][qx]);
-                    else aux_stress_plane(g0, g1, (float)c.sigma, sm.aux[qy][qx]);
+                    else aux_stress_plane(g0, g1, c.pf.sigma, sm.aux[qy][qx]);
                 } else {
                     iso_grad(sm.phi, qx + 1, qy + 1, g0, g1, g2);
                     if (tipo == ITLBM_OP_F1) aux_normal(g0, g1, g2, sm.aux[qy][qx]);
@@ -253,6 +250,8 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
 
     // ---- phase C: mediator gradient, force, collision, push ----------------------------------
     if (valid) {
+        CaseDev::F32Par pf{};  // FP32: the case's parameters in float
+        if constexpr (std::is_same<S, float>::value) pf = load_pf(c);
         const int px = lx + HMAX, py = ly + HMAX;
         S gmx, gmy, gmz;
         auto phi_at = [&](int dx, int dy) { return sm.phi[py + dy][px + dx]; };
@@ -269,7 +268,10 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                 kappa = curvature_plane([&](int dx, int dy) { return sm.aux[qy + dy][qx + dx]; });
             else
                 kappa = curvature<S, AUXS>(sm.aux, qx, qy);
-            const S hs = (S(0.5) * (S)c.sigma) * kappa;
+            S sig;
+            if constexpr (std::is_same<S, float>::value) sig = pf.sigma;
+            else sig = c.sigma;
+            const S hs = (S(0.5) * sig) * kappa;
             Fx = hs * sm.g[qy][qx][0];
             Fy = hs * sm.g[qy][qx][1];
             Fz = hs * sm.g[qy][qx][2];
@@ -284,7 +286,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                 g0 = -gmx;  // the isotropic gradient is the exact negative of the mediator momentum
                 g1 = -gmy;
                 g2 = -gmz;
-                mu = chem_pot_fold(phi_at, (float)c.kf, (float)c.bf);
+                mu = chem_pot_fold(phi_at, pf.kf, pf.bf);
             } else {
                 iso_grad(sm.phi, px, py, g0, g1, g2);
                 mu = chem_pot(sm.phi, px, py, (S)c.kf, (S)c.bf);
@@ -303,16 +305,16 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         bool skip;
         if constexpr (FOLD) {
             RecolourFold rc;
-            if (force) collide_fold<true>(f, sa, sb, gmx, gmy, Fx, Fy, c, rc);
-            else collide_fold<false>(f, sa, sb, gmx, gmy, Fx, Fy, c, rc);
+            if (force) collide_fold<true>(f, sa, sb, gmx, gmy, Fx, Fy, pf, rc);
+            else collide_fold<false>(f, sa, sb, gmx, gmy, Fx, Fy, pf, rc);
             skip = rc.skip;
             if (!skip) {
                 double dsum = 0.0;
                 sfor<0, 4>([&](auto M) {
                     constexpr int K = 2 * decltype(M)::value + 1;
                     float dK, dJ;
-                    split_fold_pair<K>(rc, f[K], f[K + 1], shift_of<kx(K)>(c, wk<float>(K)),
-                                       shift_of<kx(K + 1)>(c, wk<float>(K + 1)), dK, dJ);
+                    split_fold_pair<K>(rc, f[K], f[K + 1], shift_of<kx(K)>(pf, wk<float>(K)),
+                                       shift_of<kx(K + 1)>(pf, wk<float>(K + 1)), dK, dJ);
                     dsum += (double)dK;
                     dsum += (double)dJ;
                     float *nK = dst_node(K), *nJ = dst_node(K + 1);
@@ -342,8 +344,8 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             }
         } else {
             Recolour32 rc;
-            if (force) collide_f32<true>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
-            else collide_f32<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+            if (force) collide_f32<true>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, pf, rc);
+            else collide_f32<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, pf, rc);
             skip = rc.skip;
             if (!skip) {
                 // d_0 is the complement of the moving d_i against the incoming D, both summed in
@@ -354,8 +356,8 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                 sfor<0, 9>([&](auto M) {
                     constexpr int i = 2 * decltype(M)::value + 1;
                     float di, dj;
-                    split32_pair<i>(rc, f[i], f[i + 1], shift_of<cx(i)>(c, wgt<float>(i)),
-                                    shift_of<cx(i + 1)>(c, wgt<float>(i + 1)), di, dj);
+                    split32_pair<i>(rc, f[i], f[i + 1], shift_of<cx(i)>(pf, wgt<float>(i)),
+                                    shift_of<cx(i + 1)>(pf, wgt<float>(i + 1)), di, dj);
                     dsum += (double)di;
                     dsum += (double)dj;
                     float *ni = dst_node(i), *nj = dst_node(i + 1);

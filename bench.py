@@ -18,7 +18,8 @@ value   MLUPS (million lattice-node updates per second) of the batch, device tim
         on the batch's stream around exactly K steps, state resident in HBM (11+ GB, far larger than
         L2, so no flush is needed between steps).
 e2e     the same metric through the C ABI as a user runs the batch: itlbm_batch_submit of every case
-        (the initial profiles are computed on the host and copied up), advances of up to 500 steps
+        (a strip's initial profile is computed on the host and copied up, a drop's on the device),
+        advances of up to 500 steps
         with the diagnostics that fall due (each a device-to-host copy of the observables), wall
         clock from the first submit to the last step.
 roofline algorithmic bytes per update: 38 populations read + 38 written (304 B in FP32, 608 B in
@@ -64,8 +65,8 @@ def load_package():
 PEAKS = REPO / "MEASURED_PEAKS.json"
 # HBM traffic per node of one FP32 step launch, dram__bytes_read.sum + dram__bytes_write.sum from one
 # ncu capture each: a launch over a 100-case subset of the batch mix (1.73 GB for 5 542 507 nodes) and a
-# launch over the 4096^2 drop (5.07 GB for 16 777 216 nodes).
-TRAFFIC_B_PER_NODE = {"batch600": (912097536 + 816680704) / 5542507, "single": 5069217280 / 16777216}
+# launch over the 4096^2 drop (5.06 GB for 16 777 216 nodes).
+TRAFFIC_B_PER_NODE = {"batch600": (912193536 + 813472000) / 5542507, "single": (2552271872 + 2507548928) / 16777216}
 HBM_FALLBACK = 6650.0
 
 
@@ -221,9 +222,16 @@ def served_latency(pkg, load=0.7):
     st = b.stats()
     b.close()
     lat = np.sort(np.array(lat))
+    # HBM bytes per node update of the stream, weighted by each request's planned work: 608 B for the
+    # FP64 requests, 304 B for the FP32 ones
+    planned = [(r["nx"] ** 2 * r["steps"], 608.0 if r["fp64"] else 304.0) for r in reqs]
+    bpu = sum(w * b_ for w, b_ in planned) / sum(w for w, _ in planned)
+    peak, peak_kind = hbm_peak()
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "max_s": float(lat[-1]), "requests": len(reqs), "offered_load": load,
-            "capacity_mlups": capacity_mlups, "offered_mlups": load * capacity_mlups,
+            "capacity_mlups": capacity_mlups, "bytes_per_update": bpu,
+            "capacity_roofline_frac": capacity_mlups * 1e6 * bpu / 1e9 / peak,
+            "offered_mlups": load * capacity_mlups,
             "achieved_mlups": st.node_updates / wall / 1e6, "wall_s": wall,
             "workload": "served stream, scaled: Poisson arrivals, side 64-1024, 500-5000 steps, 10% FP64, "
                         "80% drops / 20% strips, 7 operators; offered load relative to the capacity measured "
@@ -765,7 +773,15 @@ def main():
                         "one-node slab up to rounding; reported beside, never as, the D3Q19 value"}
     e2e = None
     if not args.no_e2e:
+        # clocks sampled over the whole end-to-end run (seconds of sustained load, against the
+        # headline's short timed region): the power cap lowers the SM clock under sustained load
+        e2e_sampler = ClockSampler(local) if rank == 0 else None
+        if e2e_sampler:
+            e2e_sampler.__enter__()
         e2e = batch_e2e(pkg, 1001) if args.workload == "batch600" else e2e_run(pkg, single, pkg.PREC_F32, args.steps)
+        if e2e_sampler:
+            e2e_sampler.__exit__()
+            e2e["clocks"] = e2e_sampler.summary()
         if world > 1:
             e2e["value"] = allreduce_sum(e2e["value"], world)
     latency = latency_c5 = None

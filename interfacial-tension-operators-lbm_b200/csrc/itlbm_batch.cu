@@ -324,13 +324,14 @@ long long updates_in(const itlbm_batch *b, int k0, int k1) {
     return u;
 }
 
-// Autotuning on the first full replay, in timed windows of M = K / 16 sub-steps (CUDA events, rate
-// per node update): the tiling -- narrow tiles at the partial last tile column of a case against
+// Autotuning on the first full replay of at least 18 sub-steps, in timed windows of
+// M = max(6, K / 16) sub-steps (CUDA events, rate per node update): the tiling -- narrow tiles at the partial last tile column of a case against
 // 32 x 8 tiles throughout -- with one CTA per table entry, then persistent CTAs at the occupancy limit
 // with the better tiling.  The faster of each runs the rest of the replay and is captured into the
 // graph.  Every choice runs the same arithmetic on every node, so the results do not depend on it.
+constexpr int TUNE_MIN_WINDOW = 6;  // shorter windows were noisy enough to pick a 30 % slower tiling
 int tune_and_run(itlbm_batch *b, int K) {
-    const int M = std::max(2, K / 16);
+    const int M = std::max(TUNE_MIN_WINDOW, K / 16);
     int k0 = 0;
     auto window = [&](int mode, bool narrow, double &rate) -> int {
         if (narrow != b->narrow) {
@@ -897,7 +898,7 @@ int itlbm_batch_advance(itlbm_batch *b, void *stream) {
         b->tables_dirty = false;
     }
     cudaEventRecord(b->ev0, b->stream);
-    if (b->tuning && K == b->cfg.chunk && K >= 16) {
+    if (b->tuning && K == b->cfg.chunk && K >= 3 * TUNE_MIN_WINDOW) {
         r = tune_and_run(b, K);
         if (r) return r;
     } else if (K == b->cfg.chunk) {

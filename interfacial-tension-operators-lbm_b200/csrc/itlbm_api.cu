@@ -122,10 +122,11 @@ void case_tiles(const CaseDev &h, bool narrow_edges, int case_id, std::vector<Ti
     const int r = h.nx % TX;                               // columns of a partial last tile column
     const int edge = !narrow_edges || r == 0 ? SHAPE_32x8 : (r <= 8 ? SHAPE_8x32 : (r <= 16 ? SHAPE_16x16 : SHAPE_32x8));
     const int full = edge == SHAPE_32x8 ? h.tiles_x : h.tiles_x - 1;  // columns of 32 x 8 tiles
-    for (int ty = 0; ty < (h.ny + TY - 1) / TY; ty++)
-        for (int tx = 0; tx < full; tx++) out[SHAPE_32x8].push_back(TileRef{case_id, tile_code(tx * TX, ty * TY)});
+    const int th = TY * rows_per_thread(h.prec);  // rows of a full-width tile
+    for (int ty = 0; ty < (h.ny + th - 1) / th; ty++)
+        for (int tx = 0; tx < full; tx++) out[SHAPE_32x8].push_back(TileRef{case_id, tile_code(tx * TX, ty * th)});
     if (edge != SHAPE_32x8) {
-        const int eh = shape_h(edge);
+        const int eh = shape_h(edge) * rows_per_thread(h.prec);
         for (int y0 = 0; y0 < h.ny; y0 += eh) out[edge].push_back(TileRef{case_id, tile_code(full * TX, y0)});
     }
 }

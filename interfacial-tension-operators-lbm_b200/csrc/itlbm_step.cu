@@ -143,13 +143,15 @@ __device__ __forceinline__ void ring_pos(int r, int H, int &px, int &py) {
 //   phase B  F1 / F2: gradient and normal or stress on the ring-1 region;
 //   phase C  mediator gradient, force, collision, recolouring, push to x + c_i.
 // FOLD (FP32 only): the nine in-plane classes per colour instead of the 19 populations.
-template <class S, bool FOLD, int W, int Hh>
+template <class S, bool FOLD, int W, int Hh, int R>
 __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int aux_k,
                                           SmemT<S, W, Hh> &sm) {
     constexpr int NP = FOLD ? NK : NV;  // storage planes per colour
     constexpr int QX = SmemT<S, W, Hh>::QX, QY = SmemT<S, W, Hh>::QY;
+    constexpr int HT = Hh / R;          // rows of one pass of the CTA's threads
+    static_assert(HT * W == STEP_THREADS, "a pass of the threads covers W x HT nodes");
     const int tid = threadIdx.x;
-    const int lx = tid % W, ly = tid / W;
+    const int lx = tid % W, ly = tid / W;  // the thread's nodes are rows ly + jr HT, jr < R
     const int nx = c.nx, ny = c.ny, tiles_x = c.tiles_x;
     constexpr int TE = 2 * NP * PLANE;  // elements per tile block
     // the address of node (x, y) in a buffer; plane q of the node is at [q * PLANE] from it
@@ -164,36 +166,43 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     const float rho0f = c.pf.rho0;  // FP32: the reference density in float (phase_of)
 
     // ---- phase A ----------------------------------------------------------------------------
-    const int x = x0 + lx, y = y0 + ly;
-    const bool valid = (x < xe) && (y < ye);
-    S f[NP], sa = S(0), sb = S(0);
-    double sbd = 0.0;
-    if (x < xe + H && y < ye + H) {
-        const int xw = valid ? x : wrap_near(x, nx), yw = valid ? y : wrap_near(y, ny);
-        const S *own = node(src, xw, yw);
-        S a[NP], b[NP];
+    const int x = x0 + lx;
+    S f[R][NP], sa[R], sb[R];
+    double sbd[R];
 #pragma unroll
-        for (int i = 0; i < NP; i++) a[i] = ldg<LD_OWN>(own + i * PLANE);
+    for (int jr = 0; jr < R; jr++) {
+        const int lyj = ly + jr * HT, y = y0 + lyj;
+        const bool valid = (x < xe) && (y < ye);
+        sa[jr] = S(0);
+        sb[jr] = S(0);
+        sbd[jr] = 0.0;
+        if (x < xe + H && y < ye + H) {
+            const int xw = valid ? x : wrap_near(x, nx), yw = valid ? y : wrap_near(y, ny);
+            const S *own = node(src, xw, yw);
+            S a[NP], b[NP];
 #pragma unroll
-        for (int i = 0; i < NP; i++) b[i] = ldg<LD_OWN>(own + (NP + i) * PLANE);
+            for (int i = 0; i < NP; i++) a[i] = ldg<LD_OWN>(own + i * PLANE);
 #pragma unroll
-        for (int i = 0; i < NP; i++) sa = sa + a[i];
+            for (int i = 0; i < NP; i++) b[i] = ldg<LD_OWN>(own + (NP + i) * PLANE);
 #pragma unroll
-        for (int i = 0; i < NP; i++) sb = sb + b[i];
-        if constexpr (std::is_same<S, float>::value) {
-            // FP32: rho^N from the FP32 sums (as for the halo nodes); the colour difference is also
-            // summed in FP64 for the rest population's complement (see the split below)
+            for (int i = 0; i < NP; i++) sa[jr] = sa[jr] + a[i];
 #pragma unroll
-            for (int i = 0; i < NP; i++) sbd += (double)b[i];
+            for (int i = 0; i < NP; i++) sb[jr] = sb[jr] + b[i];
+            if constexpr (std::is_same<S, float>::value) {
+                // FP32: rho^N from the FP32 sums (as for the halo nodes); the colour difference is
+                // also summed in FP64 for the rest population's complement (see the split below)
+#pragma unroll
+                for (int i = 0; i < NP; i++) sbd[jr] += (double)b[i];
+            }
+            if constexpr (std::is_same<S, double>::value) {
+#pragma unroll
+                for (int i = 0; i < NP; i++) f[jr][i] = a[i] + b[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < NP; i++) f[jr][i] = a[i];
+            }
+            sm.phi[lyj + HMAX][lx + HMAX] = phase_of(sa[jr], sb[jr], rho0f);
         }
-        if constexpr (std::is_same<S, double>::value) {
-#pragma unroll
-            for (int i = 0; i < NP; i++) f[i] = a[i] + b[i];
-        } else {
-#pragma unroll
-            for (int i = 0; i < NP; i++) f[i] = a[i];
-        }
-        sm.phi[ly + HMAX][lx + HMAX] = phase_of(sa, sb, rho0f);
     }
     // halo ring: item it = (ring node it / 2, colour it % 2), the two colours of a node on adjacent
     // lanes, which exchange their sums by a shuffle; the loop runs in whole warps (the bound is a
@@ -249,10 +258,13 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
     }
 
     // ---- phase C: mediator gradient, force, collision, push ----------------------------------
-    if (valid) {
+#pragma unroll
+    for (int jr = 0; jr < R; jr++) {
+      const int lyj = ly + jr * HT, y = y0 + lyj;
+      if ((x < xe) && (y < ye)) {
         CaseDev::F32Par pf{};  // FP32: the case's parameters in float
         if constexpr (std::is_same<S, float>::value) pf = load_pf(c);
-        const int px = lx + HMAX, py = ly + HMAX;
+        const int px = lx + HMAX, py = lyj + HMAX;
         S gmx, gmy, gmz;
         auto phi_at = [&](int dx, int dy) { return sm.phi[py + dy][px + dx]; };
         if constexpr (std::is_same<S, float>::value) {
@@ -262,7 +274,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         S Fx = S(0), Fy = S(0), Fz = S(0);
         const bool force = tipo >= ITLBM_OP_F1;
         if (tipo == ITLBM_OP_F1) {
-            const int qx = lx + 1, qy = ly + 1;
+            const int qx = lx + 1, qy = lyj + 1;
             S kappa;
             if constexpr (std::is_same<S, float>::value)
                 kappa = curvature_plane([&](int dx, int dy) { return sm.aux[qy + dy][qx + dx]; });
@@ -277,9 +289,9 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             Fz = hs * sm.g[qy][qx][2];
         } else if (tipo == ITLBM_OP_F2) {
             if constexpr (std::is_same<S, float>::value)
-                stress_div_plane([&](int dx, int dy) { return sm.aux[ly + 1 + dy][lx + 1 + dx]; }, Fx, Fy);
+                stress_div_plane([&](int dx, int dy) { return sm.aux[lyj + 1 + dy][lx + 1 + dx]; }, Fx, Fy);
             else
-                stress_div<S, AUXS>(sm.aux, lx + 1, ly + 1, Fx, Fy, Fz);
+                stress_div<S, AUXS>(sm.aux, lx + 1, lyj + 1, Fx, Fy, Fz);
         } else if (tipo == ITLBM_OP_F3) {
             S g0, g1, g2, mu;
             if constexpr (std::is_same<S, float>::value) {
@@ -305,38 +317,38 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
         bool skip;
         if constexpr (FOLD) {
             RecolourFold rc;
-            if (force) collide_fold<true>(f, sa, sb, gmx, gmy, Fx, Fy, pf, rc);
-            else collide_fold<false>(f, sa, sb, gmx, gmy, Fx, Fy, pf, rc);
+            if (force) collide_fold<true>(f[jr], sa[jr], sb[jr], gmx, gmy, Fx, Fy, pf, rc);
+            else collide_fold<false>(f[jr], sa[jr], sb[jr], gmx, gmy, Fx, Fy, pf, rc);
             skip = rc.skip;
             if (!skip) {
                 double dsum = 0.0;
                 sfor<0, 4>([&](auto M) {
                     constexpr int K = 2 * decltype(M)::value + 1;
                     float dK, dJ;
-                    split_fold_pair<K>(rc, f[K], f[K + 1], shift_of<kx(K)>(pf, wk<float>(K)),
+                    split_fold_pair<K>(rc, f[jr][K], f[jr][K + 1], shift_of<kx(K)>(pf, wk<float>(K)),
                                        shift_of<kx(K + 1)>(pf, wk<float>(K + 1)), dK, dJ);
                     dsum += (double)dK;
                     dsum += (double)dJ;
                     float *nK = dst_node(K), *nJ = dst_node(K + 1);
-                    stg(nK + K * PLANE, f[K]);
+                    stg(nK + K * PLANE, f[jr][K]);
                     stg(nK + (NK + K) * PLANE, dK);
-                    stg(nJ + (K + 1) * PLANE, f[K + 1]);
+                    stg(nJ + (K + 1) * PLANE, f[jr][K + 1]);
                     stg(nJ + (NK + K + 1) * PLANE, dJ);
                 });
                 float *n0 = dst_node(0);
-                stg(n0, f[0]);
-                stg(n0 + NK * PLANE, (float)(sbd - dsum));
+                stg(n0, f[jr][0]);
+                stg(n0 + NK * PLANE, (float)(sbd[jr] - dsum));
             }
         } else if constexpr (std::is_same<S, double>::value) {
             Recolour64 rc;
-            if (force) collide_f64<true>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
-            else collide_f64<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+            if (force) collide_f64<true>(f[jr], sa[jr], sb[jr], gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
+            else collide_f64<false>(f[jr], sa[jr], sb[jr], gmx, gmy, gmz, Fx, Fy, Fz, c, rc);
             skip = rc.skip;
             if (!skip) {
                 sfor<0, NV>([&](auto I) {
                     constexpr int i = decltype(I)::value;
                     double r, b;
-                    split64<i>(rc, f[i], r, b);
+                    split64<i>(rc, f[jr][i], r, b);
                     double *n = dst_node(i);
                     stg(n + i * PLANE, r);
                     stg(n + (NV + i) * PLANE, b);
@@ -344,8 +356,8 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             }
         } else {
             Recolour32 rc;
-            if (force) collide_f32<true>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, pf, rc);
-            else collide_f32<false>(f, sa, sb, gmx, gmy, gmz, Fx, Fy, Fz, pf, rc);
+            if (force) collide_f32<true>(f[jr], sa[jr], sb[jr], gmx, gmy, gmz, Fx, Fy, Fz, pf, rc);
+            else collide_f32<false>(f[jr], sa[jr], sb[jr], gmx, gmy, gmz, Fx, Fy, Fz, pf, rc);
             skip = rc.skip;
             if (!skip) {
                 // d_0 is the complement of the moving d_i against the incoming D, both summed in
@@ -356,19 +368,19 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
                 sfor<0, 9>([&](auto M) {
                     constexpr int i = 2 * decltype(M)::value + 1;
                     float di, dj;
-                    split32_pair<i>(rc, f[i], f[i + 1], shift_of<cx(i)>(pf, wgt<float>(i)),
+                    split32_pair<i>(rc, f[jr][i], f[jr][i + 1], shift_of<cx(i)>(pf, wgt<float>(i)),
                                     shift_of<cx(i + 1)>(pf, wgt<float>(i + 1)), di, dj);
                     dsum += (double)di;
                     dsum += (double)dj;
                     float *ni = dst_node(i), *nj = dst_node(i + 1);
-                    stg(ni + i * PLANE, f[i]);
+                    stg(ni + i * PLANE, f[jr][i]);
                     stg(ni + (NV + i) * PLANE, di);
-                    stg(nj + (i + 1) * PLANE, f[i + 1]);
+                    stg(nj + (i + 1) * PLANE, f[jr][i + 1]);
                     stg(nj + (NV + i + 1) * PLANE, dj);
                 });
                 float *n0 = dst_node(0);
-                stg(n0, f[0]);
-                stg(n0 + NV * PLANE, (float)(sbd - dsum));
+                stg(n0, f[jr][0]);
+                stg(n0 + NV * PLANE, (float)(sbd[jr] - dsum));
             }
         }
         if (skip) {  // rho <= 1e-30: the site is streamed unchanged (Operadores_tensao.cpp:347)
@@ -389,6 +401,7 @@ __device__ __forceinline__ void step_tile(const CaseDev &c, int tile, int k, int
             c.aux[2 * n + o] = (double)Fz;
             c.aux[3 * n + o] = sqrt((double)gmx * gmx + (double)gmy * gmy + (double)gmz * gmz);
         }
+      }
     }
     __syncthreads();
 }
@@ -415,14 +428,15 @@ __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS(FOLD)) k_s
                                                        const TileRef *__restrict__ tiles,
                                                        int ntiles, const int *__restrict__ ntiles_dev,
                                                        int k, int aux_k) {
-    constexpr int Hh = STEP_THREADS / W;
+    constexpr int R = FOLD ? ITLBM_FOLD_ROWS : 1;  // rows of the tile per thread
+    constexpr int Hh = R * STEP_THREADS / W;
     __shared__ SmemT<S, W, Hh> sm;
     const int nt = ntiles_dev ? *ntiles_dev : ntiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const TileRef tr = tiles[t];
         const CaseDev &c = cases[tr.case_id];
         if (k >= c.chunk_len) continue;
-        step_tile<S, FOLD, W, Hh>(c, tr.tile, k, aux_k, sm);
+        step_tile<S, FOLD, W, Hh, R>(c, tr.tile, k, aux_k, sm);
     }
 }
 

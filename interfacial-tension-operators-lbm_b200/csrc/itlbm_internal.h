@@ -30,10 +30,17 @@ __host__ __device__ constexpr int shape_w(int s) { return s == SHAPE_32x8 ? 32 :
 __host__ __device__ constexpr int shape_h(int s) { return STEP_THREADS / shape_w(s); }
 // Rows of a tile per thread: the fold's threads take two nodes each (rows ly and ly + 256 / W), so
 // its tiles are 32 x 16 (or 16 x 32, 8 x 64 at a partial edge); the other storage forms take one.
+// Measured on B200: two rows made the fold 13 % faster; for the D3Q19 FP32 form (38 values per node)
+// they need 80-128 registers and were 7-12 % slower at 3 or 2 CTAs per SM.
 #ifndef ITLBM_FOLD_ROWS
 #define ITLBM_FOLD_ROWS 2
 #endif
-__host__ __device__ constexpr int rows_per_thread(int prec) { return prec == ITLBM_PREC_F32_FOLD ? ITLBM_FOLD_ROWS : 1; }
+#ifndef ITLBM_F32_ROWS
+#define ITLBM_F32_ROWS 1
+#endif
+__host__ __device__ constexpr int rows_per_thread(int prec) {
+    return prec == ITLBM_PREC_F32_FOLD ? ITLBM_FOLD_ROWS : (prec == ITLBM_PREC_F32 ? ITLBM_F32_ROWS : 1);
+}
 // D3Q19 velocity set in the order of def_lattice_d3q19 (SimBoltz_Functions/LBM_functions.cpp:366-497)
 __host__ __device__ constexpr int cx(int i) {
     constexpr int t[NV] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};

@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(STEP_THREADS, ITLBM_STEP_MIN_BLOCKS(FOLD)) k_s
                                                        const TileRef *__restrict__ tiles,
                                                        int ntiles, const int *__restrict__ ntiles_dev,
                                                        int k, int aux_k) {
-    constexpr int R = FOLD ? ITLBM_FOLD_ROWS : 1;  // rows of the tile per thread
+    constexpr int R = FOLD ? ITLBM_FOLD_ROWS : (std::is_same<S, float>::value ? ITLBM_F32_ROWS : 1);  // rows per thread
     constexpr int Hh = R * STEP_THREADS / W;
     __shared__ SmemT<S, W, Hh> sm;
     const int nt = ntiles_dev ? *ntiles_dev : ntiles;

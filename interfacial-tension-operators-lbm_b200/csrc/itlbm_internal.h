@@ -15,9 +15,10 @@ namespace itlbm {
 
 constexpr int NV = 19;
 
-// Tiles of the fused step: 256 interior nodes, one per thread, in one of three shapes; the phase
-// field is staged with a halo of up to HMAX nodes (1 for P1/P3/F3, 2 for F1/F2).  A case is tiled by
-// 32 x 8 tiles (a warp per row of 32 nodes); the last tile column, when nx is not a multiple of 32,
+// Tiles of the fused step: 256 threads, one node each (two in the fold, see rows_per_thread), in one
+// of three shapes; the phase field is staged with a halo of up to HMAX nodes (1 for P1/P3/F3, 2 for
+// F1/F2).  A case is tiled by 32 x 8 tiles (a warp per row of 32 nodes); the last tile column, when
+// nx is not a multiple of 32,
 // can instead be cut into 16 x 16 or 8 x 32 tiles (a warp covering 2 or 4 row pieces of 16 or 8
 // nodes), which leaves fewer threads idle beyond the box's edge.  The shape changes no result: a
 // node's update is the same whichever tile computes it.

@@ -11,9 +11,10 @@
 // `dst`, as propag_site does (SimBoltz_Functions/LBM_functions.cpp:1220-1247).  The post-collision
 // values the diagnostics need are therefore dst(x + c_i, i).
 //
-// One CTA handles a tile of 256 nodes of one case (the work table says which; its shape -- 32 x 8, or
-// 16 x 16 / 8 x 32 at the edge of a box whose width is not a multiple of 32 -- is that of the kernel).  It stages rho^N for the
-// tile plus a halo of 1 (P1, P3, F3) or 2 (F1, F2) nodes in shared memory -- the halo nodes are
+// One CTA of 256 threads handles a tile of 256 nodes (512 in the fold, two rows per thread) of one
+// case (the work table says which; its shape -- 32 x 8, or 16 x 16 / 8 x 32 at the edge of a box
+// whose width is not a multiple of 32 -- is that of the kernel).  It stages rho^N for the tile plus a
+// halo of 1 (P1, P3, F3) or 2 (F1, F2) nodes in shared memory -- the halo nodes are
 // re-read from L2, where the neighbouring tiles keep them -- then evaluates the mediator gradient,
 // the force of class F on a ring-1 region of auxiliary fields, and collides.  No mediator
 // populations or force fields ever reach HBM.

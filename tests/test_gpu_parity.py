@@ -369,7 +369,8 @@ def test_fields_need_the_force_of_class_f(gpu):
 @pytest.mark.parametrize("nx", [7, 40, 45, 61, 64, 100])
 def test_tile_shapes_agree(gpu, monkeypatch, prec, nx):
     """A partial last tile column cut into 8 x 32 (nx mod 32 <= 8) or 16 x 16 tiles (<= 16) gives the
-    same bits as 32 x 8 tiles throughout, for every storage form and both halo widths."""
+    same bits as 32 x 8 tiles throughout, for every storage form and both halo widths (the fold's
+    threads take two rows, so its tiles are 8 x 64, 16 x 32 and 32 x 16)."""
     out = {}
     for narrow in ("1", "0"):
         monkeypatch.setenv("ITLBM_NARROW_EDGES", narrow)

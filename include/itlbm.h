@@ -277,8 +277,9 @@ typedef struct itlbm_batch_stats {
                               /* the occupancy limit, k > 0 k persistent CTAs per SM               */
     int       held;           /* finished cases kept for itlbm_batch_read_fields (not in `active`) */
     int       narrow_edges;   /* tiling in use: 1 the partial last tile column of a case in 16 x 16 */
-                              /* or 8 x 32 tiles, 0 32 x 8 tiles throughout (autotuned like the    */
-                              /* launch shape; the results do not depend on it)                     */
+                              /* or 8 x 32 tiles, 0 32 x 8 tiles throughout (in the fold, two rows  */
+                              /* per thread: 16 x 32, 8 x 64 and 32 x 16); autotuned like the      */
+                              /* launch shape; the results do not depend on it                      */
 } itlbm_batch_stats;
 
 /* No case memory is allocated until cases are admitted. */

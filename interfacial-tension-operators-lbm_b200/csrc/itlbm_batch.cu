@@ -105,6 +105,8 @@ struct itlbm_batch {
         size_t off;  // of its profile in the staging buffer
     };
     std::vector<InitJob> inits;  // admitted this round, initial state not yet launched
+    std::vector<int> dev_inits;  // admitted this round, initial state formed on the device, not yet launched
+    int desc_lo = INT_MAX, desc_hi = -1;  // slots whose descriptors are not yet on the device
     std::deque<Pending> pending;
     std::vector<Active *> slots;
     std::vector<int> free_slots;
@@ -421,6 +423,17 @@ cudaError_t stage_reserve(itlbm_batch *b, size_t len) {
 // The initial profiles of the cases admitted so far in this round, filled by host threads that take
 // chunks of about 16 K nodes from all of them at once (most boxes are too small to split alone), then
 // their initial-state launches, in admission order.
+// The descriptors of the slots admitted since the last upload, in one copy on the batch stream (the
+// init kernels read them from the device).
+cudaError_t upload_descs(itlbm_batch *b) {
+    if (b->desc_hi < b->desc_lo) return cudaSuccess;
+    const int lo = b->desc_lo, hi = b->desc_hi;
+    b->desc_lo = INT_MAX;
+    b->desc_hi = -1;
+    return cudaMemcpyAsync(b->d_cases + lo, b->h_cases.data() + lo, sizeof(CaseDev) * (size_t)(hi - lo + 1),
+                           cudaMemcpyHostToDevice, b->stream);
+}
+
 cudaError_t flush_inits(itlbm_batch *b) {
     if (b->inits.empty()) return cudaSuccess;
     struct Chunk {
@@ -449,7 +462,7 @@ cudaError_t flush_inits(itlbm_batch *b) {
     for (int t = 1; t < nthr; t++) pool.emplace_back(work);
     work();
     for (auto &th : pool) th.join();
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = upload_descs(b);
     for (const auto &w : b->inits)
         if (e == cudaSuccess) e = launch_init_from(w.h, b->d_cases + w.slot, w.d, b->stage_dev + w.off, b->stream);
     b->inits.clear();
@@ -499,11 +512,12 @@ int admit_cases(itlbm_batch *b) {
         a->slot = slot;
         b->slots[slot] = a;
         b->h_cases[slot] = h;
-        // on the batch stream, which is not ordered after the legacy stream's copies
-        e = cudaMemcpyAsync(b->d_cases + slot, &h, sizeof(CaseDev), cudaMemcpyHostToDevice, b->stream);
+        // the descriptor goes up with the round's others, in one copy on the batch stream (which is
+        // not ordered after the legacy stream's copies) before any init kernel reads it
+        b->desc_lo = std::min(b->desc_lo, slot);
+        b->desc_hi = std::max(b->desc_hi, slot);
         if (p.snapshot.empty() && profile_on_device(d)) {
-            if (e == cudaSuccess) e = launch_init_from(h, b->d_cases + slot, d, nullptr, b->stream);
-            if (e != cudaSuccess) return cuda_fail(e, "admission");
+            b->dev_inits.push_back(slot);
         } else if (p.snapshot.empty()) {
             const size_t len = profile_len(h, d);
             // a full staging buffer is reused only after the profiles queued in it are launched
@@ -515,6 +529,7 @@ int admit_cases(itlbm_batch *b) {
             }
             if (e != cudaSuccess) return cuda_fail(e, "admission");
         } else {
+            e = upload_descs(b);
             if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
             if (e != cudaSuccess) return cuda_fail(e, "admission");
             const int r = snap_read_state(p.snapshot.c_str(), h, h.buf[0]);
@@ -530,7 +545,14 @@ int admit_cases(itlbm_batch *b) {
 
 int admit(itlbm_batch *b) {
     const int r = admit_cases(b);
-    const cudaError_t e = flush_inits(b);
+    // the descriptors first, then the init kernels that form their states on the device
+    cudaError_t e = upload_descs(b);
+    for (const int slot : b->dev_inits) {
+        const Active *a = b->slots[slot];
+        if (e == cudaSuccess && a) e = launch_init_from(b->h_cases[slot], b->d_cases + slot, a->desc, nullptr, b->stream);
+    }
+    b->dev_inits.clear();
+    if (e == cudaSuccess) e = flush_inits(b);
     if (r) return r;
     return e == cudaSuccess ? ITLBM_OK : cuda_fail(e, "initial states");
 }

@@ -115,3 +115,51 @@ def test_fold_strip_and_batch(gpu):
             alone = c.diag_drop(250).as_dict()
         for key in ("massa_R", "u_max", "raio", "delta_p"):
             assert alone[key] == rows[(k, 250)][key], (k, key)
+
+
+
+@pytest.mark.parametrize("nx,ny", [(37, 29), (20, 17), (45, 40), (64, 23)])
+@pytest.mark.parametrize("tipo,A", [(3, 0.05), (12, 0.05)], ids=["P3", "F2"])
+def test_fold_small_and_ragged_boxes(gpu, nx, ny, tipo, A):
+    """The fold's threads take two rows of a 32 x 16 tile: boxes narrower or lower than one tile, and
+    heights that leave the second row of a tile's threads partly outside the box, follow the FP64
+    path as the 19-population FP32 storage does.  (Drops of radius ~2 in boxes of 5-9 rows are left to
+    the next test: their symmetric states put interface nodes at points where the phase gradient is
+    rounding noise, and the recolouring direction taken there separates every FP32 storage from the
+    FP64 path by ~1e-3 within two steps.)"""
+    op = gpu.make_op(tipo, 0.5, 1.569988)
+    cs = [gpu.Case(gpu.desc(nx, ny, op, tau=0.8, A_fact=A, radius=min(nx, ny) / 4.0,
+                            k_profile=2.0 * math.log(9.0) / 3.45, precision=p))
+          for p in (gpu.PREC_F64, gpu.PREC_F32, gpu.PREC_F32_FOLD)]
+    try:
+        for c in cs:
+            c.step(120)
+        ref = fold(cs[0].read_pops(0))
+        assert np.isfinite(ref).all()
+        err_f32 = np.abs(fold(cs[1].read_pops(0)) - ref).max()
+        err_fold = np.abs(fold(cs[2].read_pops(0)) - ref).max()
+        assert err_fold <= max(4 * err_f32, 2e-6), (err_fold, err_f32)
+    finally:
+        for c in cs:
+            c.close()
+
+
+@pytest.mark.parametrize("nx,ny", [(7, 5), (33, 9), (12, 20)])
+@pytest.mark.parametrize("tipo,A", [(3, 0.05), (12, 0.05)], ids=["P3", "F2"])
+def test_fold_tiny_boxes_tilings_agree(gpu, monkeypatch, nx, ny, tipo, A):
+    """Boxes smaller than one tile, where the halo of both of a thread's rows wraps inside the tile:
+    the fold gives the same bits with 32 x 16 tiles throughout and with the partial column cut into
+    narrow 8 x 64 / 16 x 32 tiles (two different placements of every node in its tile's rows)."""
+    op = gpu.make_op(tipo, 0.5, 1.569988)
+    out = {}
+    for narrow in ("1", "0"):
+        monkeypatch.setenv("ITLBM_NARROW_EDGES", narrow)
+        c = gpu.Case(gpu.desc(nx, ny, op, tau=0.8, A_fact=A, radius=max(2.0, min(nx, ny) / 4.0),
+                              k_profile=2.0 * math.log(9.0) / 3.45, precision=gpu.PREC_F32_FOLD))
+        try:
+            c.step(60)
+            out[narrow] = c.read_pops(0)
+        finally:
+            c.close()
+    assert np.isfinite(out["0"][0]).all()
+    assert all(np.array_equal(a, b) for a, b in zip(out["1"], out["0"]))
